@@ -1,0 +1,181 @@
+"""GPU parity: the CUDA library (through the C ABI) against the CPU FP64 oracle and the
+reference's golden results. Tolerances are written in each test:
+
+* FP64 local operators and apply: relative 1e-12 (same FP64 mathematics, different summation
+  order and the reference GPU's exact edge moments instead of edge quadrature);
+* FP32 operator: relative 2e-6 of the FP64 result;
+* solutions: relative 2-norm difference to the oracle's sparse-LU solution, given per test from
+  the solve tolerance;
+* golden error figures: the oracle's own tolerances (tests/test_oracle_golden.py).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import vemgpu  # noqa: E402
+from vemgpu import meshgen  # noqa: E402
+
+GEO = {O.GEOM_IDENTITY: "identity", O.GEOM_SINE: "sine", O.GEOM_ARCS: "arcs"}
+PROB = {O.PROB_SINCOS: "sincos", O.PROB_SINSIN: "sinsin", O.PROB_ANNULUS: "annulus"}
+BCN = {O.BC_FLUX: "flux", O.BC_PRESSURE: "pressure"}
+
+
+def pair(mesh, k, nq, geom, eps, problem, bc, theta=None, ng=9):
+    o = O.Oracle(mesh, k=k, nq=nq, ng=ng, geom=geom, eps=eps, problem=problem, bc=bc, theta=theta)
+    g = vemgpu.DarcyGpu(mesh, k=k, nq=nq, ng=ng, geometry=GEO[geom], eps=eps, problem=PROB[problem], bc=BCN[bc],
+                        theta=theta)
+    assert (g.nc, g.ne, g.nf, g.np, g.N) == (o.nc, o.ne, o.nf, o.np, o.N)
+    return o, g
+
+
+@pytest.fixture(scope="module")
+def disk200():
+    return meshgen.voronoi_mesh(200, "disk", seed=3)
+
+
+@pytest.fixture(scope="module")
+def annulus300():
+    return meshgen.voronoi_mesh(300, "annulus", seed=4)
+
+
+def _close(a, b, rtol):
+    scale = max(np.abs(b).max(), 1e-300)
+    assert np.abs(a - b).max() <= rtol * scale, (np.abs(a - b).max() / scale)
+
+
+LOCAL_CASES = [
+    ("square_2x2", 0, 9, O.GEOM_SINE, 0.05, O.BC_FLUX),
+    ("square_2x2", 1, 9, O.GEOM_SINE, 0.05, O.BC_FLUX),
+    ("square_2x2", 2, 9, O.GEOM_SINE, 0.05, O.BC_FLUX),
+    ("square_1x1", 3, 12, O.GEOM_SINE, 0.05, O.BC_FLUX),
+    ("square_1x1", 4, 36, O.GEOM_IDENTITY, 0.0, O.BC_FLUX),
+]
+
+
+@pytest.mark.parametrize("name,k,nq,geom,eps,bc", LOCAL_CASES)
+def test_local_operators_square(square_meshes, name, k, nq, geom, eps, bc):
+    o, g = pair(square_meshes[name], k, nq, geom, eps, O.PROB_SINCOS, bc)
+    for c in range(o.nc):
+        n = len(o.local(c, "dir"))
+        _close(g.local(c, "A"), o.local(c, "A"), 1e-12)
+        _close(g.local(c, "P"), o.local(c, "P"), 1e-11)
+        _close(g.local(c, "W"), o.local(c, "W") if k else np.ones(n), 1e-13)
+        _close(g.local(c, "alpha"), o.local(c, "alpha"), 1e-13)
+        _close(g.local(c, "rhs"), o.local(c, "rhs"), 1e-12)
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_local_operators_arcs(disk200, k):
+    th = np.random.default_rng(5).normal(0, 1, 200)
+    o, g = pair(disk200, k, 9, O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE, theta=th)
+    for c in range(0, o.nc, 7):
+        _close(g.local(c, "A"), o.local(c, "A"), 1e-12)
+        _close(g.local(c, "rhs"), o.local(c, "rhs"), 1e-12)
+        _close(g.local(c, "dload"), o.local(c, "dload"), 1e-12)
+
+
+def _apply_case(o, g, constrained):
+    K, _ = o.system()
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal(o.N)
+    y = g.apply(torch.from_numpy(x).cuda(), constrained=constrained).cpu().numpy()
+    if constrained and o.bc == O.BC_FLUX:
+        mask, _ = o.boundary()
+        xq = np.where(mask, 0.0, x)
+        ref = K @ xq
+        ref[mask] = x[mask]
+    else:
+        ref = K @ x
+    return x, y, ref
+
+
+@pytest.mark.parametrize("name,k", [("square_4x4", 0), ("square_4x4", 1), ("square_2x2", 2)])
+@pytest.mark.parametrize("constrained", [False, True])
+def test_apply_matches_oracle_csr(square_meshes, name, k, constrained):
+    o, g = pair(square_meshes[name], k, 9, O.GEOM_SINE, 0.05, O.PROB_SINCOS, O.BC_FLUX)
+    x, y, ref = _apply_case(o, g, constrained)
+    _close(y, ref, 1e-12)
+    y32 = g.apply(torch.from_numpy(x).float().cuda(), constrained=constrained).double().cpu().numpy()
+    _close(y32, ref, 2e-6)
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_apply_arcs_pressure_bc(disk200, k):
+    o, g = pair(disk200, k, 9, O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
+    x, y, ref = _apply_case(o, g, True)
+    _close(y, ref, 1e-12)
+    _, b = o.system()
+    _close(g.rhs().cpu().numpy(), b, 1e-12)
+
+
+def test_apply_is_deterministic(disk200):
+    _, g = pair(disk200, 0, 9, O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
+    x = torch.randn(g.N, dtype=torch.float64, device="cuda")
+    a = g.apply(x)
+    for _ in range(3):
+        assert torch.equal(a, g.apply(x))
+
+
+def test_golden_reports_on_gpu(golden, square_meshes):
+    for r in golden["reports"]:
+        s = vemgpu.DarcySolver(square_meshes[r["mesh"]], problem=r["example"], gauss_point_num=r["nq"],
+                               gauss_point_num_1d=9, k=r["k"])
+        assert s.getTotalDofFlux() + s.getTotalDofConc() + 1 == r["dofs"]
+        s.solve(tol=1e-12)
+        e = s._errors()
+        tol = 1e-7 if r["k"] == 4 else 2e-9
+        for key in ("scalar_comp", "flux_comp", "scalar_phys", "flux_phys", "div_phys"):
+            assert e[key] == pytest.approx(r["values"][key], rel=tol), (r["source"], key)
+        assert abs(e["mass"] - r["values"]["mass"]) < 1e-8
+
+
+@pytest.mark.parametrize("name,k", [("square_8x8", 1), ("square_4x4", 2), ("square_8x8", 0)])
+def test_solution_matches_oracle_flux_bc(square_meshes, name, k):
+    o, g = pair(square_meshes[name], k, 9, O.GEOM_SINE, 0.05, O.PROB_SINCOS, O.BC_FLUX)
+    xo, _, _ = o.solve_direct()
+    x, info = g.solve(tol=1e-12)
+    assert info["residual"] <= 1e-12
+    xg = x.cpu().numpy()
+    assert np.linalg.norm(xg - xo) <= 1e-9 * np.linalg.norm(xo)
+    eo, eg = o.errors(xo), g.errors(x)
+    for key in eo:
+        assert eg[key] == pytest.approx(eo[key], rel=1e-8, abs=1e-12), key
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_solution_matches_oracle_disk(k):
+    m = meshgen.voronoi_mesh(1000, "disk", seed=2)
+    o, g = pair(m, k, 9, O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
+    xo, _, _ = o.solve_direct()
+    x, info = g.solve(tol=1e-10)
+    assert info["residual"] <= 1e-10
+    xg = x.cpu().numpy()
+    assert np.linalg.norm(xg - xo) <= 1e-8 * np.linalg.norm(xo)
+    # the error kernel reproduces the oracle's figures on the same vector
+    eo, eg = o.errors(xg), g.errors(x)
+    for key in eo:
+        assert eg[key] == pytest.approx(eo[key], rel=1e-11, abs=1e-14), key
+
+
+def test_mixed_precision_refinement(annulus300):
+    th = np.random.default_rng(7).normal(0, 2, 300)
+    o, g = pair(annulus300, 0, 9, O.GEOM_ARCS, 0.0, O.PROB_ANNULUS, O.BC_PRESSURE, theta=th)
+    x64, i64 = g.solve(tol=1e-10, mode="fp64")
+    xm, im = g.solve(tol=1e-10, mode="mixed")
+    assert i64["residual"] <= 1e-10 and im["residual"] <= 1e-10
+    xo, _, _ = o.solve_direct()
+    for x in (x64, xm):
+        assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+
+
+def test_solve_host_matches_device(annulus300):
+    _, g = pair(annulus300, 0, 9, O.GEOM_ARCS, 0.0, O.PROB_ANNULUS, O.BC_PRESSURE)
+    b = g.rhs()
+    xd, _ = g.solve(b)
+    xh, info = g.solve_host(b.cpu().numpy())
+    assert info["residual"] <= 1e-10
+    assert np.array_equal(xd.cpu().numpy(), xh)

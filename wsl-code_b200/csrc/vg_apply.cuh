@@ -1,0 +1,34 @@
+// Matrix-free apply: argument block and launcher.
+#pragma once
+#include <vector>
+
+#include "vg_common.cuh"
+
+namespace vg {
+
+template <typename T>
+struct ApplyArgs {
+    const T* x;
+    T* y;               // flux edge entries must be zero on entry (atomic scatter)
+    const T* A;         // packed A_E, slot-major per bucket
+    const T* W;         // W_E (k >= 1), slot-major per bucket
+    const int* map;     // signed flux dof map, slot-major per bucket
+    const int* slot_cell;
+    const T* L;         // multiplier vector per cell (q), when mult
+    const int* mask;    // essential-BC mask (N), when constrained
+    const int* flags;   // optional: skip when flags[0] != 0
+    long long nf, N;
+    T psign;
+    int constrained, mult;
+    double* partials;   // 2 per block, when red or mult
+    unsigned int* counter;
+    double* red;        // optional: quadratic form x^T K x -> red[0]
+    int total_blocks, block_off;
+};
+
+int apply_blocks(const std::vector<Bucket>& buckets);
+
+template <typename T>
+void launch_apply(ApplyArgs<T> a, const std::vector<Bucket>& buckets, int k, cudaStream_t s);
+
+}  // namespace vg

@@ -1,0 +1,212 @@
+// C ABI of vemgpu (include/vemgpu.h). Every entry point converts exceptions into status codes;
+// no C++ exception crosses the boundary (the rule of vem/CurvedVEM_Darcy_gpu/src/krylov.cu:8-36).
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "vemgpu.h"
+#include "vg_solver.hpp"
+
+struct vg_handle {
+    std::unique_ptr<vg::Solver> s;
+    std::string error;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(vg_handle* h, F f) {
+    if (!h || !h->s) return VG_EINVAL;
+    try {
+        f(*h->s);
+        h->error.clear();
+        return VG_OK;
+    } catch (const vg::Error& e) {
+        h->error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        h->error = "host allocation failed";
+        return VG_ENOMEM;
+    } catch (const std::exception& e) {
+        h->error = e.what();
+        return VG_EINVAL;
+    }
+}
+
+int create(vg::HostMesh&& m, const vg_geometry* g, int k, int nq, int ng, int device, vg_handle** out) {
+    auto h = std::make_unique<vg_handle>();
+    h->s = std::make_unique<vg::Solver>(std::move(m), g, k, nq, ng, device);
+    *out = h.release();
+    return VG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int vg_create(const vg_mesh* mesh, const vg_geometry* geometry, int k, int nq, int ng, int device, vg_handle** out) {
+    if (!out) return VG_EINVAL;
+    *out = nullptr;
+    try {
+        if (!mesh) throw vg::Error(VG_EINVAL, "null mesh");
+        vg::HostMesh m;
+        vg::copy_processed(m, *mesh);
+        return create(std::move(m), geometry, k, nq, ng, device, out);
+    } catch (const vg::Error& e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return VG_EINVAL;
+    }
+}
+
+int vg_create_polygons(int num_nodes, const double* node_coords, int num_cells, const int* cell_ptr,
+                       const int* cell_nodes, const vg_geometry* geometry, int k, int nq, int ng, int device,
+                       vg_handle** out) {
+    if (!out) return VG_EINVAL;
+    *out = nullptr;
+    try {
+        vg::HostMesh m;
+        vg::process_polygons(m, num_nodes, node_coords, num_cells, cell_ptr, cell_nodes);
+        return create(std::move(m), geometry, k, nq, ng, device, out);
+    } catch (const vg::Error& e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return VG_EINVAL;
+    }
+}
+
+int vg_destroy(vg_handle* h) {
+    delete h;
+    return VG_OK;
+}
+
+const char* vg_last_error(const vg_handle* h) { return h ? h->error.c_str() : g_create_error.c_str(); }
+
+int vg_sizes(const vg_handle* h, long long out[9]) {
+    if (!h || !h->s || !out) return VG_EINVAL;
+    const auto& s = *h->s;
+    out[0] = s.m.nc;
+    out[1] = s.m.ne;
+    out[2] = s.nf;
+    out[3] = s.np;
+    out[4] = s.N;
+    out[5] = s.q;
+    out[6] = s.p;
+    out[7] = s.internal;
+    out[8] = s.maxn;
+    return VG_OK;
+}
+
+int vg_set_problem(vg_handle* h, int problem, int bc) {
+    return guarded(h, [&](vg::Solver& s) { s.set_problem(problem, bc); });
+}
+
+int vg_set_log_permeability(vg_handle* h, const double* theta, int on_device) {
+    return guarded(h, [&](vg::Solver& s) { s.set_theta(theta, on_device != 0); });
+}
+
+int vg_build(vg_handle* h) {
+    return guarded(h, [&](vg::Solver& s) { s.build(); });
+}
+
+int vg_apply(vg_handle* h, const void* x, void* y, int precision, int constrained, void* stream) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!s.built) throw vg::Error(VG_ESTATE, "vg_build must run before vg_apply");
+        if (!x || !y || x == y) throw vg::Error(VG_EINVAL, "apply requires distinct non-null vectors");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (precision == VG_FP64) {
+            VG_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * s.N, st));
+            s.apply64(static_cast<const double*>(x), static_cast<double*>(y), constrained != 0, 1.0, st);
+        } else if (precision == VG_FP32) {
+            VG_CUDA(cudaMemsetAsync(y, 0, sizeof(float) * s.N, st));
+            s.apply32(static_cast<const float*>(x), static_cast<float*>(y), constrained != 0, 1.0f, st);
+        } else {
+            throw vg::Error(VG_EINVAL, "precision must be VG_FP64 or VG_FP32");
+        }
+    });
+}
+
+int vg_rhs(vg_handle* h, double* b) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!s.built) throw vg::Error(VG_ESTATE, "vg_build must run before vg_rhs");
+        if (!b) throw vg::Error(VG_EINVAL, "null vector");
+        s.rhs(b, nullptr);
+        VG_CUDA(cudaDeviceSynchronize());
+    });
+}
+
+void vg_default_solve_opts(vg_solve_opts* o) {
+    if (!o) return;
+    o->mode = VG_SOLVE_FP64;
+    o->tol = 1e-10;
+    o->maxit = 200000;
+    o->inner_tol = 1e-5;
+    o->max_outer = 12;
+    o->check_every = 32;
+    o->nonzero_guess = 0;
+}
+
+int vg_solve(vg_handle* h, const double* b, double* x, const vg_solve_opts* opts, vg_solve_info* info) {
+    return guarded(h, [&](vg::Solver& s) {
+        vg_solve_opts o;
+        vg_default_solve_opts(&o);
+        if (opts) o = *opts;
+        vg_solve_info inf{};
+        try {
+            s.solve(b, x, o, inf, nullptr);
+        } catch (...) {
+            if (info) *info = inf;
+            throw;
+        }
+        if (info) *info = inf;
+    });
+}
+
+int vg_solve_host(vg_handle* h, const double* b_host, double* x_host, const vg_solve_opts* opts, vg_solve_info* info) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!b_host || !x_host) throw vg::Error(VG_EINVAL, "null vector");
+        vg_solve_opts o;
+        vg_default_solve_opts(&o);
+        if (opts) o = *opts;
+        vg::DevBuf<double> b(s.N), x(s.N);
+        VG_CUDA(cudaMemcpy(b.data(), b_host, sizeof(double) * s.N, cudaMemcpyHostToDevice));
+        if (o.nonzero_guess) VG_CUDA(cudaMemcpy(x.data(), x_host, sizeof(double) * s.N, cudaMemcpyHostToDevice));
+        vg_solve_info inf{};
+        s.solve(b.data(), x.data(), o, inf, nullptr);
+        VG_CUDA(cudaMemcpy(x_host, x.data(), sizeof(double) * s.N, cudaMemcpyDeviceToHost));
+        if (info) *info = inf;
+    });
+}
+
+int vg_adjoint_grad(vg_handle* h, const double* x, const double* dJdx, double* dJdtheta, const vg_solve_opts* opts,
+                    vg_solve_info* info) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!x || !dJdx || !dJdtheta) throw vg::Error(VG_EINVAL, "null vector");
+        vg_solve_opts o;
+        vg_default_solve_opts(&o);
+        if (opts) o = *opts;
+        vg_solve_info inf{};
+        s.adjoint(x, dJdx, dJdtheta, o, inf, nullptr);
+        if (info) *info = inf;
+    });
+}
+
+int vg_errors(vg_handle* h, const double* x, double out[6]) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!x || !out) throw vg::Error(VG_EINVAL, "null vector");
+        s.errors(x, out, nullptr);
+    });
+}
+
+int vg_local(vg_handle* h, int cell, int which, double* out, int* count) {
+    return guarded(h, [&](vg::Solver& s) {
+        int c = s.local(cell, which, out);
+        if (count) *count = c;
+    });
+}
+
+}  // extern "C"

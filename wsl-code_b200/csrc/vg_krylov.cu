@@ -1,0 +1,248 @@
+// Preconditioned MINRES (Paige-Saunders, in the form with unnormalised Lanczos vectors and a
+// symmetric positive definite preconditioner) on the symmetric saddle-point system
+//     [A, -W^T; -W, 0] [u; p] = [g; -f],
+// replacing the PETSc FGMRES of vem/CurvedVEM_Darcy_gpu/src/krylov.cu:49-175. Per iteration:
+//   (a) apply        y = K z_j and delta_j = z_j^T K z_j (fused, vg_apply.cu)
+//   (b) update       v_{j+1} = y/g_j - (delta_j/g_j^2) v_j - (g_j/g_{j-1}) v_{j-1},
+//                    z_{j+1} = P^{-1} v_{j+1}, gamma_{j+1} = sqrt(z_{j+1}.v_{j+1}), clear y,
+//                    Givens rotation, residual estimate (last block, device scalars)
+//   (c) step         w_{j+1} = (z_j/g_j - a3 w_{j-1} - a2 w_j)/a1, x += c_{j+1} eta_j w_{j+1}
+// All scalars stay on the device; convergence sets a stop flag that turns the remaining kernels
+// of a batch into no-ops, so iterations run without host synchronisation. Every reduction is a
+// fixed-shape two-level sum (block partials, last block sums them in order): results are
+// bitwise reproducible.
+#include "vg_krylov.cuh"
+
+namespace vg {
+
+namespace {
+
+// block + grid reduction of NV values; the last block to finish calls fin(total)
+template <int NV, class F>
+__device__ void grid_reduce(double (&v)[NV], double* partials, unsigned* counter, F fin) {
+    __shared__ double sh[VEC_THREADS / 32][NV];
+    __shared__ double tot[VEC_THREADS][NV];
+    __shared__ bool last;
+    const int t = threadIdx.x, w = t >> 5, l = t & 31;
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+        for (int off = 16; off; off >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
+    if (l == 0)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) sh[w][i] = v[i];
+    __syncthreads();
+    if (t == 0) {
+        for (int i = 0; i < NV; ++i) {
+            double s = 0;
+            for (int k = 0; k < VEC_THREADS / 32; ++k) s += sh[k][i];
+            partials[NV * blockIdx.x + i] = s;
+        }
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = 0;
+    for (int b = t; b < (int)gridDim.x; b += VEC_THREADS)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) acc[i] += __ldcg(partials + NV * b + i);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) tot[t][i] = acc[i];
+    __syncthreads();
+    for (int s = VEC_THREADS / 2; s; s >>= 1) {
+        if (t < s)
+#pragma unroll
+            for (int i = 0; i < NV; ++i) tot[t][i] += tot[t + s][i];
+        __syncthreads();
+    }
+    if (t == 0) {
+        double r[NV];
+        for (int i = 0; i < NV; ++i) r[i] = tot[0][i];
+        fin(r);
+        *counter = 0u;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_init(const T* r, MinresVecs<T> v, long long n, Scalars* sc,
+                                                      int* flags, double tol, double* partials, unsigned* counter) {
+    double acc[1] = {0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        T ri = r[i], zi = v.dinv[i] * ri;
+        v.v_cur[i] = ri;
+        v.v_old[i] = T(0);
+        v.z_cur[i] = zi;
+        v.w_cur[i] = T(0);
+        v.w_old[i] = T(0);
+        v.y[i] = T(0);
+        acc[0] += double(zi) * double(ri);
+    }
+    grid_reduce<1>(acc, partials, counter, [&](double* tot) {
+        double g = sqrt(fmax(tot[0], 0.0));
+        sc->gam = g;
+        sc->gam_prev = 1.0;
+        sc->c_prev = 1.0;
+        sc->c = 1.0;
+        sc->s_prev = 0.0;
+        sc->s = 0.0;
+        sc->eta = g;
+        sc->eta0 = g;
+        sc->tol = tol;
+        flags[0] = (g > 0 && isfinite(g)) ? 0 : 1;
+        flags[1] = 0;
+        flags[2] = 0;
+    });
+}
+
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags,
+                                                        double* partials, unsigned* counter) {
+    if (flags[0]) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) flags[1] = 0;
+        return;
+    }
+    const double g = sc->gam, gp = sc->gam_prev, dl = sc->delta / (g * g);
+    const T f1 = T(1.0 / g), f2 = T(dl / g), f3 = T(g / gp);
+    double acc[1] = {0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        T vn = v.y[i] * f1 - f2 * v.v_cur[i] - f3 * v.v_old[i];
+        T zn = v.dinv[i] * vn;
+        v.v_old[i] = vn;
+        v.z_new[i] = zn;
+        v.y[i] = T(0);
+        acc[0] += double(zn) * double(vn);
+    }
+    grid_reduce<1>(acc, partials, counter, [&](double* tot) {
+        double gn = sqrt(fmax(tot[0], 0.0));
+        double c = sc->c, cp = sc->c_prev, s = sc->s, sp = sc->s_prev, eta = sc->eta;
+        double a0 = c * dl - cp * s * g;
+        double a1 = sqrt(a0 * a0 + gn * gn);
+        double a2 = s * dl + cp * c * g;
+        double a3 = sp * g;
+        bool ok = a1 > 0 && isfinite(a1);
+        double cn = ok ? a0 / a1 : 1.0, sn = ok ? gn / a1 : 0.0;
+        sc->a1 = ok ? a1 : 1.0;
+        sc->a2 = a2;
+        sc->a3 = a3;
+        sc->zscale = 1.0 / g;
+        sc->xcoef = ok ? cn * eta : 0.0;
+        sc->eta = -sn * eta;
+        sc->c_prev = c;
+        sc->c = cn;
+        sc->s_prev = s;
+        sc->s = sn;
+        sc->gam_prev = g;
+        sc->gam = gn;
+        flags[1] = ok ? 1 : 0;
+        flags[2] += 1;
+        if (!ok || !(gn > 0) || fabs(sc->eta) <= sc->tol * sc->eta0) flags[0] = 1;
+    });
+}
+
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_step(MinresVecs<T> v, long long n, Scalars* sc, int* flags) {
+    if (!flags[1]) return;
+    const T zs = T(sc->zscale), a2 = T(sc->a2), a3 = T(sc->a3), ia1 = T(1.0 / sc->a1), xc = T(sc->xcoef);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        T wn = (v.z_cur[i] * zs - a3 * v.w_old[i] - a2 * v.w_cur[i]) * ia1;
+        v.w_old[i] = wn;
+        v.x[i] += xc * wn;
+    }
+}
+
+__global__ void __launch_bounds__(VEC_THREADS) k_residual64(const double* b, const double* y, double* r, long long n,
+                                                            double* red, double* partials, unsigned* counter) {
+    double acc[2] = {0, 0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double bi = b[i], ri = bi - y[i];
+        r[i] = ri;
+        acc[0] += ri * ri;
+        acc[1] += bi * bi;
+    }
+    grid_reduce<2>(acc, partials, counter, [&](double* tot) {
+        red[0] = tot[0];
+        red[1] = tot[1];
+    });
+}
+
+__global__ void k_to_float(const double* in, float* out, double scale, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = float(scale * in[i]);
+}
+
+__global__ void k_axpy_from_float(double* x, const float* d, double scale, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] += scale * double(d[i]);
+}
+
+__global__ void k_flip(const double* in, double* out, long long nf, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = i < nf ? in[i] : -in[i];
+}
+
+__global__ void k_to_float_plain(const double* in, float* out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = float(in[i]);
+}
+
+}  // namespace
+
+template <typename T>
+void minres_init(const T* r, MinresVecs<T> v, long long n, Scalars* sc, int* flags, double tol, double* partials,
+                 unsigned* counter, cudaStream_t s) {
+    k_init<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(r, v, n, sc, flags, tol, partials, counter);
+    VG_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void minres_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags, double* partials, unsigned* counter,
+                   cudaStream_t s) {
+    k_update<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(v, n, sc, flags, partials, counter);
+    VG_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void minres_step(MinresVecs<T> v, long long n, Scalars* sc, int* flags, cudaStream_t s) {
+    k_step<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(v, n, sc, flags);
+    VG_CUDA(cudaGetLastError());
+}
+
+template void minres_init<double>(const double*, MinresVecs<double>, long long, Scalars*, int*, double, double*,
+                                  unsigned*, cudaStream_t);
+template void minres_init<float>(const float*, MinresVecs<float>, long long, Scalars*, int*, double, double*,
+                                 unsigned*, cudaStream_t);
+template void minres_update<double>(MinresVecs<double>, long long, Scalars*, int*, double*, unsigned*, cudaStream_t);
+template void minres_update<float>(MinresVecs<float>, long long, Scalars*, int*, double*, unsigned*, cudaStream_t);
+template void minres_step<double>(MinresVecs<double>, long long, Scalars*, int*, cudaStream_t);
+template void minres_step<float>(MinresVecs<float>, long long, Scalars*, int*, cudaStream_t);
+
+void residual64(const double* b, const double* y, double* r, long long n, double* red, double* partials,
+                unsigned* counter, cudaStream_t s) {
+    k_residual64<<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(b, y, r, n, red, partials, counter);
+    VG_CUDA(cudaGetLastError());
+}
+
+void to_float(const double* in, float* out, double scale, long long n, cudaStream_t s) {
+    k_to_float<<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(in, out, scale, n);
+    VG_CUDA(cudaGetLastError());
+}
+
+void axpy_from_float(double* x, const float* d, double scale, long long n, cudaStream_t s) {
+    k_axpy_from_float<<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(x, d, scale, n);
+    VG_CUDA(cudaGetLastError());
+}
+
+void flip_pressure(const double* in, double* out, long long nf, long long n, cudaStream_t s) {
+    k_flip<<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(in, out, nf, n);
+    VG_CUDA(cudaGetLastError());
+}
+
+void to_float_plain(const double* in, float* out, long long n, cudaStream_t s) {
+    k_to_float_plain<<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(in, out, n);
+    VG_CUDA(cudaGetLastError());
+}
+
+}  // namespace vg

@@ -1,0 +1,765 @@
+// vemgpu Solver: host orchestration of the device setup, apply, Krylov solve, adjoint and errors.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+
+#include "vg_apply.cuh"
+#include "vg_krylov.cuh"
+#include "vg_setup.cuh"
+#include "vg_solver.hpp"
+
+namespace vg {
+
+void diag_flux(const double* A, const int* map, const Bucket& b, double* d, cudaStream_t s);
+void diag_finish(const double* A, const double* W, const int* map, const int* slot_cell, const int* mask,
+                 const double* L, const Bucket& b, int k, long long nf, double* d, double* contrib, cudaStream_t s);
+void diag_invert(double* d, const int* mask, const double* contrib, int nc, long long nf, long long np, int mult,
+                 long long N, cudaStream_t s);
+void lift_rhs(const int* mask, const double* g, const double* y, double* b, long long N, cudaStream_t s);
+void rescale_ops(const double* theta, const int* slot_cell, const Bucket& b, const double* A0, double* A64, float* A32,
+                 cudaStream_t s);
+void contract_adjoint(const double* A, const int* map, const int* slot_cell, const int* mask, const Bucket& b,
+                      const double* x, const double* mu, int constrained, double* g, cudaStream_t s);
+
+namespace {
+
+// Gauss-Legendre rules on [-1, 1] (vem/CurvedVEM_Darcy_gpu/core/gauss_quadrature.cpp:74-167)
+std::vector<double> gauss_legendre(int n) {
+    struct H {
+        double x, w;
+    };
+    std::vector<H> half;
+    bool centre = false;
+    double wc = 0;
+    switch (n) {
+    case 1: return {0.0, 2.0};
+    case 2: half = {{0.5773502691896257645091488, 1.0}}; break;
+    case 3: half = {{0.7745966692414833770358531, 0.5555555555555556}}; centre = true; wc = 0.8888888888888889; break;
+    case 4: half = {{0.8611363115940526, 0.3478548451374539}, {0.3399810435848563, 0.6521451548625461}}; break;
+    case 5:
+        half = {{0.9061798459386640, 0.2369268850561891}, {0.5384693101056831, 0.4786286704993665}};
+        centre = true;
+        wc = 0.5688888888888889;
+        break;
+    case 6:
+        half = {{0.9324695142031520, 0.1713244923791703}, {0.6612093864662645, 0.3607615730481386},
+                {0.2386191860831969, 0.4679139345726910}};
+        break;
+    case 7:
+        half = {{0.9491079123427585, 0.1294849661688697}, {0.7415311855993944, 0.2797053914892767},
+                {0.4058451513773972, 0.3818300505051190}};
+        centre = true;
+        wc = 0.4179591836734694;
+        break;
+    case 8:
+        half = {{0.9602898564975362, 0.1012285362903763}, {0.7966664774136267, 0.2223810344533745},
+                {0.5255324099163290, 0.3137066458778873}, {0.1834346424956498, 0.3626837833783620}};
+        break;
+    case 9:
+        half = {{0.9681602395076261, 0.0812743883615744}, {0.8360311073266358, 0.1806481606948574},
+                {0.6133714327005904, 0.2606106964029355}, {0.3242534234038089, 0.3123470770400028}};
+        centre = true;
+        wc = 0.3302393550012598;
+        break;
+    case 10:
+        half = {{0.9739065285171717, 0.0666713443086881}, {0.8650633666889845, 0.1494513491505806},
+                {0.6794095682990244, 0.2190863625159820}, {0.4333953941292472, 0.2692667193099964},
+                {0.1488743389816312, 0.2955242247147529}};
+        break;
+    default: throw Error(VG_EINVAL, "Gauss-Legendre order must be 1..10");
+    }
+    std::vector<double> out;
+    for (auto& h : half) {
+        out.push_back(-h.x);
+        out.push_back(h.w);
+    }
+    if (centre) {
+        out.push_back(0.0);
+        out.push_back(wc);
+    }
+    for (auto it = half.rbegin(); it != half.rend(); ++it) {
+        out.push_back(it->x);
+        out.push_back(it->w);
+    }
+    return out;
+}
+
+// triangle rules as (xi, eta, w) on the reference triangle (gauss_quadrature.cpp:258-305) and the
+// 36-point Duffy rule of vem/CurvedVEM_Darcy_gpu/src/mesh_pack.cpp:110-124 written the same way
+std::vector<double> triangle_rule(int n) {
+    std::vector<double> r;
+    auto add = [&](double a, double b, double w) {
+        r.push_back(a);
+        r.push_back(b);
+        r.push_back(w);
+    };
+    switch (n) {
+    case 1: add(1.0 / 3.0, 1.0 / 3.0, 0.5); break;
+    case 3:
+        add(0.5, 0.0, 1.0 / 6.0);
+        add(0.5, 0.5, 1.0 / 6.0);
+        add(0.0, 0.5, 1.0 / 6.0);
+        break;
+    case 4: {
+        double s = 1.0 / std::sqrt(3.0);
+        add((1 + s) / 2, (1 - s) * (1 + s) / 4, (1 - s) / 8.0);
+        add((1 + s) / 2, (1 - s) * (1 - s) / 4, (1 - s) / 8.0);
+        add((1 - s) / 2, (1 + s) * (1 + s) / 4, (1 + s) / 8.0);
+        add((1 - s) / 2, (1 + s) * (1 - s) / 4, (1 + s) / 8.0);
+        break;
+    }
+    case 7: {
+        add(1.0 / 3.0, 1.0 / 3.0, 0.1125);
+        double a = 0.797426985353087, b = 0.101286507323456, w1 = 0.0629695902724135;
+        add(a, b, w1);
+        add(b, a, w1);
+        add(b, b, w1);
+        double c = 0.059715871789770, d = 0.470142064105115, w2 = 0.0661970763907399;
+        add(c, d, w2);
+        add(d, c, w2);
+        add(d, d, w2);
+        break;
+    }
+    case 9: {
+        double s = std::sqrt(3.0 / 5.0);
+        add(0.5, 0.25, 64.0 / 81.0 * 1.0 / 8.0);
+        add((1 + s) / 2, (1 - s) * (1 + s) / 4, 100.0 / 324.0 * (1 - s) / 8.0);
+        add((1 + s) / 2, (1 - s) * (1 - s) / 4, 100.0 / 324.0 * (1 - s) / 8.0);
+        add((1 - s) / 2, (1 + s) * (1 + s) / 4, 100.0 / 324.0 * (1 + s) / 8.0);
+        add((1 - s) / 2, (1 + s) * (1 - s) / 4, 100.0 / 324.0 * (1 + s) / 8.0);
+        add(0.5, (1 + s) / 4, 40.0 / 81.0 * 1.0 / 8.0);
+        add(0.5, (1 - s) / 4, 40.0 / 81.0 * 1.0 / 8.0);
+        add((1 + s) / 2, (1 - s) / 4, 40.0 / 81.0 * (1 - s) / 8.0);
+        add((1 - s) / 2, (1 + s) / 4, 40.0 / 81.0 * (1 + s) / 8.0);
+        break;
+    }
+    case 12: {
+        const double a = 0.5611400349004341, b = 0.2194299825497830, wa = 0.1713331241529811 * 0.5;
+        const double c = 0.0397240717755698, d = 0.4801379641122151, wc = 0.0807310895930309 * 0.5;
+        const double e = 0.0193717243612408, f = 0.1416190159239682, g = 0.8390092597147911,
+                     we = 0.0406345597936607 * 0.5;
+        add(a, b, wa);
+        add(b, b, wa);
+        add(b, a, wa);
+        add(c, d, wc);
+        add(d, d, wc);
+        add(d, c, wc);
+        add(e, f, we);
+        add(f, g, we);
+        add(g, e, we);
+        add(f, e, we);
+        add(e, g, we);
+        add(g, f, we);
+        break;
+    }
+    case 36: {
+        auto g6 = gauss_legendre(6);
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 6; ++j) {
+                double u = (g6[2 * i] + 1) / 2, wa = g6[2 * i + 1] / 2, ub = (g6[2 * j] + 1) / 2, wb = g6[2 * j + 1] / 2;
+                add(u, (1 - u) * ub, wa * wb * (1 - u));
+            }
+        break;
+    }
+    default: throw Error(VG_EINVAL, "triangle quadrature must be 1, 3, 4, 7, 9, 12 or 36");
+    }
+    return r;
+}
+
+}  // namespace
+
+Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_, int device) : m(std::move(mesh)) {
+    // option rules of vem/CurvedVEM_Darcy_gpu/src/solver_options.cpp:123-136
+    if (k_ < 0 || k_ > 4) throw Error(VG_EINVAL, "polynomial degree k must be 0..4");
+    if (nq_ != 1 && nq_ != 3 && nq_ != 4 && nq_ != 7 && nq_ != 9 && nq_ != 12 && nq_ != 36)
+        throw Error(VG_EINVAL, "triangle quadrature must be 1, 3, 4, 7, 9, 12 or 36");
+    if ((k_ >= 1 && nq_ == 1) || (k_ >= 2 && (nq_ == 3 || nq_ == 4)))
+        throw Error(VG_EINVAL, "triangle quadrature under-integrates this degree");
+    if ((k_ == 3 && nq_ < 12) || (k_ == 4 && nq_ != 36))
+        throw Error(VG_EINVAL, "insufficient triangle quadrature for this degree");
+    if (ng_ < k_ + 2 || ng_ > 10) throw Error(VG_EINVAL, "edge quadrature must be between k+2 and 10");
+    k = k_;
+    nq = nq_;
+    ng = ng_;
+    int ndev = 0;
+    VG_CUDA(cudaGetDeviceCount(&ndev));
+    if (ndev == 0) throw Error(VG_ECUDA, "no CUDA device");
+    if (device >= 0) VG_CUDA(cudaSetDevice(device));
+    VG_CUDA(cudaGetDevice(&device_));
+    q = dimP(k);
+    p = p_of(k);
+    ngrad = ngrad_of(k);
+    internal = internal_of(k);
+    nf = m.ne * (k + 1) + m.nc * internal;
+    np = m.nc * q;
+    N = nf + np + 1;  // flux BC (reference default) until set_problem
+    // geometry
+    std::vector<int> edge_arc(m.ne, -1);
+    std::vector<double> arcdata;
+    if (geo) {
+        geom_kind = geo->kind;
+        eps = geo->eps;
+        if (geom_kind < VG_GEOM_IDENTITY || geom_kind > VG_GEOM_ARCS) throw Error(VG_EINVAL, "unknown geometry kind");
+        if (geom_kind == VG_GEOM_ARCS) {
+            if (geo->num_arcs < 0 || (geo->num_arcs > 0 && (!geo->arc_nodes || !geo->arc_circles)))
+                throw Error(VG_EINVAL, "arc geometry needs arc_nodes and arc_circles");
+            std::unordered_map<unsigned long long, int> look;
+            look.reserve(size_t(m.ne) * 2);
+            for (int e = 0; e < m.ne; ++e)
+                look[(static_cast<unsigned long long>(unsigned(m.eend[2 * e])) << 32) | unsigned(m.eend[2 * e + 1])] = e;
+            arcdata.assign(3 * size_t(m.ne), 0.0);
+            for (int a = 0; a < geo->num_arcs; ++a) {
+                unsigned u = unsigned(geo->arc_nodes[2 * a]), v = unsigned(geo->arc_nodes[2 * a + 1]);
+                auto it = look.find((static_cast<unsigned long long>(std::min(u, v)) << 32) | std::max(u, v));
+                if (it == look.end()) throw Error(VG_EINVAL, "arc chord is not a mesh edge");
+                if (m.eocc[it->second] != 1) throw Error(VG_EINVAL, "arc chord is not a boundary edge");
+                if (!(geo->arc_circles[3 * a + 2] > 0)) throw Error(VG_EINVAL, "arc radius must be positive");
+                edge_arc[it->second] = a;
+                for (int c = 0; c < 3; ++c) arcdata[3 * size_t(it->second) + c] = geo->arc_circles[3 * a + c];
+            }
+        }
+    }
+    std::vector<char> curved(m.nc, 0);
+    if (geom_kind == VG_GEOM_ARCS)
+        for (int c = 0; c < m.nc; ++c)
+            for (int j = m.cptr[c]; j < m.cptr[c + 1]; ++j)
+                if (edge_arc[m.gedges[j]] >= 0) curved[c] = 1;
+    std::vector<int> triptr;
+    std::vector<TriIdx> tris;
+    triangulate(m, curved, edge_arc, triptr, tris);
+    pack_layout();
+    // uploads
+    d_xy_.upload(m.xy);
+    d_cptr_.upload(m.cptr);
+    d_cnodes_.upload(m.cnodes);
+    d_gedges_.upload(m.gedges);
+    d_cx_.upload(m.cx);
+    d_cy_.upload(m.cy);
+    d_diam_.upload(m.diam);
+    d_triptr_.upload(triptr);
+    d_tris_.upload(tris);
+    if (geom_kind == VG_GEOM_ARCS) d_arc_.upload(arcdata);
+    d_slot_cell_.upload(slot_cell_);
+    d_map_.upload(map_host_);
+    {
+        std::vector<int> occ(m.eocc);
+        DevBuf<int> tmp;
+        tmp.upload(occ);
+        d_eocc_ = std::move(tmp);
+    }
+    theta_.assign(m.nc, 0.0);
+    d_theta_.upload(theta_);
+    d_status_.resize(1);
+    d_counter_.resize(1);
+    d_counter_.zero();
+    VG_CUDA(cudaEventCreate(&ev0_));
+    VG_CUDA(cudaEventCreate(&ev1_));
+}
+
+Solver::~Solver() {
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+}
+
+void Solver::pack_layout() {
+    // buckets by edge count (ascending), cells in increasing id inside a bucket
+    std::vector<std::vector<int>> byne(MAX_NE + 1);
+    for (int c = 0; c < m.nc; ++c) byne[m.cptr[c + 1] - m.cptr[c]].push_back(c);
+    buckets_.clear();
+    slot_cell_.clear();
+    cell_slot_.assign(m.nc, -1);
+    long long slot = 0;
+    a_total_ = w_total_ = map_total_ = p_total_ = hw_total_ = 0;
+    maxn = 0;
+    for (int ne = 3; ne <= MAX_NE; ++ne) {
+        if (byne[ne].empty()) continue;
+        Bucket b{};
+        b.ne = ne;
+        b.n = (k + 1) * ne + internal;
+        b.count = int(byne[ne].size());
+        b.slot = slot;
+        b.a_off = a_total_;
+        b.w_off = w_total_;
+        b.map_off = map_total_;
+        b.p_off = p_total_;
+        b.hw_off = hw_total_;
+        long long cnt = b.count;
+        a_total_ += cnt * (b.n * (b.n + 1) / 2);
+        w_total_ += k >= 1 ? cnt * q * b.n : 0;
+        map_total_ += cnt * b.n;
+        p_total_ += cnt * p * b.n;
+        hw_total_ += cnt * q * b.n;
+        maxn = std::max(maxn, b.n);
+        for (int c : byne[ne]) {
+            cell_slot_[c] = int(slot_cell_.size());
+            slot_cell_.push_back(c);
+        }
+        slot += cnt;
+        buckets_.push_back(b);
+    }
+    // signed flux dof map (vem/CurvedVEM_Darcy_gpu/src/mesh_pack.cpp:209-225): edge moments degree-major,
+    // sign -1 on even moments of an interior edge traversed against its (min, max) orientation
+    map_host_.assign(map_total_, 0);
+    for (const auto& b : buckets_) {
+        for (int j = 0; j < b.count; ++j) {
+            int c = slot_cell_[b.slot + j];
+            int base = m.cptr[c];
+            for (int r = 0; r <= k; ++r)
+                for (int e = 0; e < b.ne; ++e) {
+                    int ge = m.gedges[base + e];
+                    int g = r * m.ne + ge;
+                    bool rev = m.cnodes[base + e] != m.eend[2 * ge];
+                    bool neg = m.eocc[ge] == 2 && rev && r % 2 == 0;
+                    map_host_[b.map_off + (long long)(r * b.ne + e) * b.count + j] = neg ? ~g : g;
+                }
+            for (int i = 0; i < internal; ++i)
+                map_host_[b.map_off + (long long)((k + 1) * b.ne + i) * b.count + j] =
+                    m.ne * (k + 1) + c * internal + i;
+        }
+    }
+}
+
+void Solver::set_problem(int problem_, int bc_) {
+    if (problem_ < VG_PROBLEM_SINCOS || problem_ > VG_PROBLEM_ANNULUS) throw Error(VG_EINVAL, "unknown problem");
+    if (bc_ != VG_BC_FLUX && bc_ != VG_BC_PRESSURE) throw Error(VG_EINVAL, "unknown boundary condition");
+    problem = problem_;
+    bc = bc_;
+    N = nf + np + (bc == VG_BC_FLUX ? 1 : 0);
+    built = false;
+}
+
+void Solver::set_theta(const double* theta, bool on_device) {
+    if (!theta) throw Error(VG_EINVAL, "null theta");
+    if (on_device)
+        VG_CUDA(cudaMemcpy(d_theta_.data(), theta, sizeof(double) * m.nc, cudaMemcpyDeviceToDevice));
+    else
+        VG_CUDA(cudaMemcpy(d_theta_.data(), theta, sizeof(double) * m.nc, cudaMemcpyHostToDevice));
+    if (built) {
+        for (const auto& b : buckets_)
+            rescale_ops(d_theta_.data(), d_slot_cell_.data(), b, d_A0_.data(), d_A64_.data(), d_A32_.data(), nullptr);
+        make_diagonal(nullptr);
+        VG_CUDA(cudaDeviceSynchronize());
+    }
+}
+
+void Solver::check_status(const char* where) {
+    unsigned long long st = 0;
+    VG_CUDA(cudaMemcpy(&st, d_status_.data(), sizeof(st), cudaMemcpyDeviceToHost));
+    if (!st) return;
+    unsigned long long code = st >> 40;
+    int cell = int(st & 0xffffffffull);
+    if (code == ST_JACOBIAN)
+        throw Error(VG_EGEOMETRY, std::string(where) + ": nonpositive Jacobian in cell " + std::to_string(cell));
+    throw Error(VG_ESINGULAR, std::string(where) + ": singular local matrix in cell " + std::to_string(cell));
+}
+
+void Solver::build() {
+    upload_rules(triangle_rule(nq), gauss_legendre(ng));
+    const int nqp = nq;
+    d_A0_.resize(a_total_);
+    d_A64_.resize(a_total_);
+    d_A32_.resize(a_total_);
+    d_W64_.resize(std::max<long long>(w_total_, 1));
+    d_W32_.resize(std::max<long long>(w_total_, 1));
+    d_P_.resize(p_total_);
+    d_HW_.resize(hw_total_);
+    d_L_.resize(size_t(m.nc) * q);
+    d_L32_.resize(size_t(m.nc) * q);
+    d_alpha_.resize(m.nc);
+    d_rhs_.resize(N);
+    d_bval_.resize(N);
+    d_mask_.resize(N);
+    d_rhs_.zero();
+    d_bval_.zero();
+    d_mask_.zero();
+    d_status_.zero();
+    SetupArgs a{};
+    a.xy = d_xy_.data();
+    a.cptr = d_cptr_.data();
+    a.cnodes = d_cnodes_.data();
+    a.gedges = d_gedges_.data();
+    a.eocc = d_eocc_.data();
+    a.cx = d_cx_.data();
+    a.cy = d_cy_.data();
+    a.diam = d_diam_.data();
+    a.triptr = d_triptr_.data();
+    a.tris = d_tris_.data();
+    a.arc = geom_kind == VG_GEOM_ARCS ? d_arc_.data() : nullptr;
+    a.slot_cell = d_slot_cell_.data();
+    a.map = d_map_.data();
+    a.theta = d_theta_.data();
+    a.k = k;
+    a.q = q;
+    a.p = p;
+    a.ngrad = ngrad;
+    a.internal = internal;
+    a.nqp = nqp;
+    a.ng = ng;
+    a.geom = geom_kind;
+    a.problem = problem;
+    a.bc = bc;
+    a.nf = nf;
+    a.eps = eps;
+    a.A0 = d_A0_.data();
+    a.A64 = d_A64_.data();
+    a.A32 = d_A32_.data();
+    a.W64 = d_W64_.data();
+    a.W32 = d_W32_.data();
+    a.P = d_P_.data();
+    a.HW = d_HW_.data();
+    a.L = d_L_.data();
+    a.L32 = d_L32_.data();
+    a.alpha = d_alpha_.data();
+    a.rhs = d_rhs_.data();
+    a.bval = d_bval_.data();
+    a.mask = d_mask_.data();
+    a.status = d_status_.data();
+    setup_args_ = a;
+    for (const auto& b : buckets_) launch_setup(a, b, nqp, nullptr);
+    VG_CUDA(cudaDeviceSynchronize());
+    check_status("setup");
+    // workspaces
+    d_partials_.resize(2 * size_t(std::max(apply_blocks(buckets_), VEC_BLOCKS)) + 16);
+    d_red_.resize(8);
+    d_scal_.resize(sizeof(Scalars) / sizeof(double) + 1);
+    d_flags_.resize(NFLAGS);
+    for (int i = 0; i < 8; ++i) {
+        w64_[i].resize(N);
+        w32_[i].resize(N);
+    }
+    d_dinv64_.resize(N);
+    d_dinv32_.resize(N);
+    make_diagonal(nullptr);
+    // BC_FLUX: lifted right-hand side of MixedGpu::make_rhs (equation_gpu.cu:611-625):
+    // free rows b - A g (unconstrained apply of the boundary values), boundary rows g
+    if (bc == VG_BC_FLUX) {
+        double* y = w64_[0].data();
+        w64_[0].zero();
+        apply64(d_bval_.data(), y, false, 1.0, nullptr);
+        lift_rhs(d_mask_.data(), d_bval_.data(), y, d_rhs_.data(), N, nullptr);
+    }
+    VG_CUDA(cudaDeviceSynchronize());
+    built = true;
+}
+
+void Solver::make_diagonal(cudaStream_t s) {
+    // SPD block-diagonal preconditioner: flux  diag(A) assembled (1 on masked dofs),
+    // pressure sum_i W_ri^2 / diag(A)_i, multiplier sum_E sum_r L_r^2 / S_rr
+    // (the diagonal of vem/CurvedVEM_Darcy_gpu/src/equation_gpu.cu:282-315 with |.| of the Schur part)
+    DevBuf<double> contrib(m.nc);
+    d_dinv64_.zero(s);
+    for (const auto& b : buckets_) diag_flux(d_A64_.data(), d_map_.data(), b, d_dinv64_.data(), s);
+    for (const auto& b : buckets_)
+        diag_finish(d_A64_.data(), d_W64_.data(), d_map_.data(), d_slot_cell_.data(),
+                    bc == VG_BC_FLUX ? d_mask_.data() : nullptr, d_L_.data(), b, k, nf, d_dinv64_.data(),
+                    contrib.data(), s);
+    diag_invert(d_dinv64_.data(), bc == VG_BC_FLUX ? d_mask_.data() : nullptr, contrib.data(), m.nc, nf, np,
+                bc == VG_BC_FLUX, N, s);
+    to_float_plain(d_dinv64_.data(), d_dinv32_.data(), N, s);
+    VG_CUDA(cudaStreamSynchronize(s));
+}
+
+void Solver::apply64(const double* x, double* y, bool constrained, double psign, cudaStream_t s, double* quad) {
+    ApplyArgs<double> a{};
+    a.x = x;
+    a.y = y;
+    a.A = d_A64_.data();
+    a.W = d_W64_.data();
+    a.map = d_map_.data();
+    a.slot_cell = d_slot_cell_.data();
+    a.L = d_L_.data();
+    a.mask = d_mask_.data();
+    a.flags = nullptr;
+    a.nf = nf;
+    a.N = N;
+    a.psign = psign;
+    a.constrained = (constrained && bc == VG_BC_FLUX) ? 1 : 0;
+    a.mult = bc == VG_BC_FLUX ? 1 : 0;
+    a.partials = d_partials_.data();
+    a.counter = d_counter_.data();
+    a.red = quad;
+    launch_apply(a, buckets_, k, s);
+}
+
+void Solver::apply32(const float* x, float* y, bool constrained, float psign, cudaStream_t s, double* quad) {
+    ApplyArgs<float> a{};
+    a.x = x;
+    a.y = y;
+    a.A = d_A32_.data();
+    a.W = d_W32_.data();
+    a.map = d_map_.data();
+    a.slot_cell = d_slot_cell_.data();
+    a.L = d_L32_.data();
+    a.mask = d_mask_.data();
+    a.flags = nullptr;
+    a.nf = nf;
+    a.N = N;
+    a.psign = psign;
+    a.constrained = (constrained && bc == VG_BC_FLUX) ? 1 : 0;
+    a.mult = bc == VG_BC_FLUX ? 1 : 0;
+    a.partials = d_partials_.data();
+    a.counter = d_counter_.data();
+    a.red = quad;
+    launch_apply(a, buckets_, k, s);
+}
+
+void Solver::rhs(double* b, cudaStream_t s) {
+    VG_CUDA(cudaMemcpyAsync(b, d_rhs_.data(), sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+}
+
+// MINRES on the symmetric constrained system K_sym x = r (x starts at zero)
+void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, int check_every, int& iters,
+                    cudaStream_t s) {
+    Scalars* sc = reinterpret_cast<Scalars*>(d_scal_.data());
+    int* flags = d_flags_.data();
+    const bool cons = bc == VG_BC_FLUX;
+    int h_flags[NFLAGS] = {0, 0, 0, 0};
+    if (fp32) {
+        MinresVecs<float> v{w32_[0].data(), w32_[1].data(), w32_[2].data(), w32_[3].data(),
+                            w32_[4].data(), w32_[5].data(), w32_[6].data(), static_cast<float*>(x),
+                            d_dinv32_.data()};
+        VG_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * N, s));
+        minres_init<float>(static_cast<const float*>(r), v, N, sc, flags, tol, d_partials_.data(), d_counter_.data(), s);
+        int done = 0;
+        while (done < maxit) {
+            int batch = std::min(check_every, maxit - done);
+            for (int it = 0; it < batch; ++it) {
+                ApplyArgs<float> a{};
+                a.x = v.z_cur;
+                a.y = v.y;
+                a.A = d_A32_.data();
+                a.W = d_W32_.data();
+                a.map = d_map_.data();
+                a.slot_cell = d_slot_cell_.data();
+                a.L = d_L32_.data();
+                a.mask = d_mask_.data();
+                a.flags = flags;
+                a.nf = nf;
+                a.N = N;
+                a.psign = -1.0f;
+                a.constrained = cons;
+                a.mult = cons;
+                a.partials = d_partials_.data();
+                a.counter = d_counter_.data();
+                a.red = &sc->delta;
+                launch_apply(a, buckets_, k, s);
+                minres_update<float>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s);
+                minres_step<float>(v, N, sc, flags, s);
+                std::swap(v.v_cur, v.v_old);
+                std::swap(v.z_cur, v.z_new);
+                std::swap(v.w_cur, v.w_old);
+            }
+            done += batch;
+            VG_CUDA(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, s));
+            VG_CUDA(cudaStreamSynchronize(s));
+            if (h_flags[0]) break;
+        }
+    } else {
+        MinresVecs<double> v{w64_[0].data(), w64_[1].data(), w64_[2].data(), w64_[3].data(),
+                             w64_[4].data(), w64_[5].data(), w64_[6].data(), static_cast<double*>(x),
+                             d_dinv64_.data()};
+        VG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
+        minres_init<double>(static_cast<const double*>(r), v, N, sc, flags, tol, d_partials_.data(), d_counter_.data(), s);
+        int done = 0;
+        while (done < maxit) {
+            int batch = std::min(check_every, maxit - done);
+            for (int it = 0; it < batch; ++it) {
+                ApplyArgs<double> a{};
+                a.x = v.z_cur;
+                a.y = v.y;
+                a.A = d_A64_.data();
+                a.W = d_W64_.data();
+                a.map = d_map_.data();
+                a.slot_cell = d_slot_cell_.data();
+                a.L = d_L_.data();
+                a.mask = d_mask_.data();
+                a.flags = flags;
+                a.nf = nf;
+                a.N = N;
+                a.psign = -1.0;
+                a.constrained = cons;
+                a.mult = cons;
+                a.partials = d_partials_.data();
+                a.counter = d_counter_.data();
+                a.red = &sc->delta;
+                launch_apply(a, buckets_, k, s);
+                minres_update<double>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s);
+                minres_step<double>(v, N, sc, flags, s);
+                std::swap(v.v_cur, v.v_old);
+                std::swap(v.z_cur, v.z_new);
+                std::swap(v.w_cur, v.w_old);
+            }
+            done += batch;
+            VG_CUDA(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, s));
+            VG_CUDA(cudaStreamSynchronize(s));
+            if (h_flags[0]) break;
+        }
+    }
+    iters = h_flags[2];
+}
+
+void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_info& info, cudaStream_t s) {
+    if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_solve");
+    if (!b || !x) throw Error(VG_EINVAL, "null vector");
+    if (!(o.tol > 0) || o.maxit < 1 || o.check_every < 1) throw Error(VG_EINVAL, "invalid solve options");
+    info = vg_solve_info{};
+    VG_CUDA(cudaEventRecord(ev0_, s));
+    const bool cons = bc == VG_BC_FLUX;
+    // symmetric form: pressure / multiplier rows negated
+    DevBuf<double> bs(N), r(N), y(N), d(N);
+    flip_pressure(b, bs.data(), nf, N, s);
+    if (!o.nonzero_guess) VG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
+    double h_red[2] = {0, 0};
+    auto true_residual = [&]() {
+        y.zero(s);
+        apply64(x, y.data(), cons, -1.0, s);
+        residual64(bs.data(), y.data(), r.data(), N, d_red_.data(), d_partials_.data(), d_counter_.data(), s);
+        VG_CUDA(cudaMemcpyAsync(h_red, d_red_.data(), sizeof(h_red), cudaMemcpyDeviceToHost, s));
+        VG_CUDA(cudaStreamSynchronize(s));
+        double nb = std::sqrt(h_red[1]);
+        return std::sqrt(h_red[0]) / (nb > 0 ? nb : 1.0);
+    };
+    double rel = true_residual();
+    int total = 0, outer = 0;
+    const double nb = std::sqrt(h_red[1]) > 0 ? std::sqrt(h_red[1]) : 1.0;
+    if (o.mode == VG_SOLVE_FP64) {
+        // MINRES in FP64 to 0.1 tol (the reference's KSP tolerance factor, krylov.cu:142), then the
+        // true FP64 residual decides; at most two restarts from the current iterate (krylov.cu:136-170)
+        for (outer = 0; outer < 3 && rel > o.tol && total < o.maxit; ++outer) {
+            int it = 0;
+            double rn = rel * nb;
+            minres(false, r.data(), d.data(), std::min(0.5, 0.1 * o.tol * nb / rn), o.maxit - total, o.check_every, it, s);
+            total += it;
+            axpy64(x, d.data(), 1.0, s);
+            rel = true_residual();
+        }
+    } else {
+        DevBuf<float> r32(N), d32(N);
+        for (outer = 0; outer < o.max_outer && rel > o.tol && total < o.maxit; ++outer) {
+            double rn = rel * nb;
+            to_float(r.data(), r32.data(), 1.0 / rn, N, s);
+            int it = 0;
+            minres(true, r32.data(), d32.data(), o.inner_tol, o.maxit - total, o.check_every, it, s);
+            total += it;
+            axpy_from_float(x, d32.data(), rn, N, s);
+            rel = true_residual();
+        }
+    }
+    VG_CUDA(cudaEventRecord(ev1_, s));
+    VG_CUDA(cudaEventSynchronize(ev1_));
+    float ms = 0;
+    VG_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    info.iterations = total;
+    info.outer = outer;
+    info.residual = rel;
+    info.seconds = ms * 1e-3;
+    if (!(rel <= o.tol))
+        throw Error(VG_ENOCONV, "Krylov solve did not converge: iterations=" + std::to_string(total) +
+                                    " true_relative_residual=" + std::to_string(rel));
+}
+
+void Solver::axpy64(double* x, const double* d, double a, cudaStream_t s) {
+    axpy64_kernel_launch(x, d, a, N, s);
+}
+
+void Solver::adjoint(const double* x, const double* dJdx, double* g, const vg_solve_opts& o, vg_solve_info& info,
+                     cudaStream_t s) {
+    if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_adjoint_grad");
+    // K_ref^T lambda = dJ/dx  <=>  K_sym mu = dJ/dx with mu = S lambda (S = diag(I, -I));
+    // solve() takes a reference-sign right-hand side b and solves K_sym x = S b, so pass S dJ/dx
+    DevBuf<double> rhs(N), mu(N);
+    flip_pressure(dJdx, rhs.data(), nf, N, s);
+    vg_solve_opts oo = o;
+    oo.nonzero_guess = 0;
+    solve(rhs.data(), mu.data(), oo, info, s);
+    // dJ/dtheta_E = -lambda^T (dK/dtheta_E) x = mu_u,E^T A_E(theta) x_u,E  (dA_E/dtheta_E = -A_E)
+    for (const auto& b : buckets_)
+        contract_adjoint(d_A64_.data(), d_map_.data(), d_slot_cell_.data(), d_mask_.data(), b, x, mu.data(),
+                         bc == VG_BC_FLUX, g, s);
+    VG_CUDA(cudaStreamSynchronize(s));
+}
+
+void Solver::errors(const double* x, double out[6], cudaStream_t s) {
+    if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_errors");
+    DevBuf<double> per(6 * size_t(m.nc)), sum(6);
+    for (const auto& b : buckets_) launch_errors(setup_args_, b, nq, x, per.data(), s);
+    launch_error_sum(per.data(), m.nc, sum.data(), s);
+    VG_CUDA(cudaMemcpyAsync(out, sum.data(), 6 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    VG_CUDA(cudaStreamSynchronize(s));
+}
+
+int Solver::local(int cell, int which, double* out) {
+    if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_local");
+    if (cell < 0 || cell >= m.nc) throw Error(VG_EINVAL, "cell out of range");
+    int slot = cell_slot_[cell];
+    const Bucket* bk = nullptr;
+    for (const auto& b : buckets_)
+        if (slot >= b.slot && slot < b.slot + b.count) bk = &b;
+    const Bucket& b = *bk;
+    long long j = slot - b.slot, mcount = b.count;
+    int n = b.n;
+    auto strided = [&](const double* base, long long off, int cnt, std::vector<double>& v) {
+        v.resize(cnt);
+        for (int e = 0; e < cnt; ++e)
+            VG_CUDA(cudaMemcpy(&v[e], base + off + e * mcount + j, sizeof(double), cudaMemcpyDeviceToHost));
+    };
+    std::vector<double> v;
+    switch (which) {
+    case 0: {
+        std::vector<double> pk;
+        strided(d_A64_.data(), b.a_off, n * (n + 1) / 2, pk);
+        v.assign(size_t(n) * n, 0.0);
+        int e = 0;
+        for (int i = 0; i < n; ++i)
+            for (int c = i; c < n; ++c) {
+                v[size_t(i) * n + c] = pk[e];
+                v[size_t(c) * n + i] = pk[e];
+                ++e;
+            }
+        break;
+    }
+    case 1:
+        if (k == 0)
+            v.assign(n, 1.0);
+        else
+            strided(d_W64_.data(), b.w_off, q * n, v);
+        break;
+    case 2: strided(d_P_.data(), b.p_off, p * n, v); break;
+    case 3: {
+        double a = 0;
+        VG_CUDA(cudaMemcpy(&a, d_alpha_.data() + cell, sizeof(double), cudaMemcpyDeviceToHost));
+        v.assign(1, a);
+        break;
+    }
+    case 4: {
+        v.resize(n);
+        for (int i = 0; i < n; ++i) {
+            int g = map_host_[b.map_off + i * mcount + j];
+            v[i] = g < 0 ? -double(~g + 1) : double(g + 1);
+        }
+        break;
+    }
+    case 5: {
+        v.resize(q);
+        VG_CUDA(cudaMemcpy(v.data(), d_rhs_.data() + nf + (long long)cell * q, q * sizeof(double), cudaMemcpyDeviceToHost));
+        break;
+    }
+    case 6: {
+        v.assign(n, 0.0);
+        if (bc == VG_BC_PRESSURE)
+            for (int i = 0; i < (k + 1) * b.ne; ++i) {
+                int g = map_host_[b.map_off + i * mcount + j];
+                int e = m.gedges[m.cptr[cell] + i % b.ne];
+                if (m.eocc[e] == 1)
+                    VG_CUDA(cudaMemcpy(&v[i], d_rhs_.data() + g, sizeof(double), cudaMemcpyDeviceToHost));
+            }
+        break;
+    }
+    default: throw Error(VG_EINVAL, "unknown local quantity");
+    }
+    if (out) std::copy(v.begin(), v.end(), out);
+    return int(v.size());
+}
+
+}  // namespace vg

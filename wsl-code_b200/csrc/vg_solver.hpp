@@ -1,0 +1,108 @@
+// Internal C++ object behind the vemgpu C ABI (one per vg_handle).
+//
+// Host side: the processed mesh (the reference reader's StraightMeshData), per-cell
+// triangulations, the degree-of-freedom map with orientation signs and the edge-count buckets
+// (the reference's HostMesh, vem/CurvedVEM_Darcy_gpu/src/mesh_pack.cpp:127-238, without the
+// per-point samples: quadrature points are generated on the device).
+// Device side: FP64 setup outputs in bucket-slot-major layout (coalesced for one thread per
+// cell), FP64 and FP32 copies of the packed local operators, Krylov workspaces.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "vg_common.cuh"
+#include "vg_setup.cuh"
+
+namespace vg {
+
+struct HostMesh {
+    int nn = 0, nc = 0, ne = 0;
+    std::vector<double> xy;
+    std::vector<int> cptr, cnodes, gedges, eend, eocc;
+    std::vector<double> cx, cy, diam;
+};
+
+// reader post-processing of raw polygons (straight_mesh.cpp:467-664)
+void process_polygons(HostMesh& m, int nn, const double* xy, int nc, const int* ptr, const int* nodes);
+// copy and validate an already processed mesh
+void copy_processed(HostMesh& m, const vg_mesh& in);
+// triangulation: reference ear clipping (decisions in cell-scaled coordinates) or, for cells with
+// an arc edge, the fan from the vertex average
+void triangulate(const HostMesh& m, const std::vector<char>& cell_curved, const std::vector<int>& edge_arc,
+                 std::vector<int>& triptr, std::vector<TriIdx>& tris);
+
+class Solver {
+public:
+    Solver(HostMesh&& mesh, const vg_geometry* geo, int k, int nq, int ng, int device);
+    ~Solver();
+
+    // configuration
+    void set_problem(int problem, int bc);
+    void set_theta(const double* theta, bool on_device);
+    void build();
+
+    // operator: y = K x (reference sign when psign = +1, symmetric when psign = -1)
+    void apply64(const double* x, double* y, bool constrained, double psign, cudaStream_t s, double* quad = nullptr);
+    void apply32(const float* x, float* y, bool constrained, float psign, cudaStream_t s, double* quad = nullptr);
+    void rhs(double* b, cudaStream_t s);
+    void solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_info& info, cudaStream_t s);
+    void adjoint(const double* x, const double* dJdx, double* g, const vg_solve_opts& o, vg_solve_info& info,
+                 cudaStream_t s);
+    void errors(const double* x, double out[6], cudaStream_t s);
+    int local(int cell, int which, double* out);
+
+    // sizes
+    int k, nq, ng, q, p, ngrad, internal, nf, np, N, maxn;
+    int problem = VG_PROBLEM_SINCOS, bc = VG_BC_FLUX;
+    bool built = false;
+    std::string error;
+
+    HostMesh m;
+    int geom_kind = VG_GEOM_IDENTITY;
+    double eps = 0;
+
+private:
+    void pack_layout();
+    void setup_kernels();
+    void rescale(cudaStream_t s);
+    void make_diagonal(cudaStream_t s);
+    void check_status(const char* where);
+    void axpy64(double* x, const double* d, double a, cudaStream_t s);
+    void minres(bool fp32, const void* b, void* x, double tol, int maxit, int check_every, int& iters,
+                cudaStream_t s);
+
+    int device_ = 0;
+    std::vector<Bucket> buckets_;
+    std::vector<int> slot_cell_;   // slot -> cell
+    std::vector<int> cell_slot_;   // cell -> slot
+    std::vector<int> map_host_;    // slot-major signed map (~g for negative orientation)
+    std::vector<double> theta_;
+    long long a_total_ = 0, w_total_ = 0, map_total_ = 0, p_total_ = 0, hw_total_ = 0;
+
+    // mesh / geometry on the device
+    DevBuf<double> d_xy_, d_cx_, d_cy_, d_diam_, d_arc_;
+    DevBuf<int> d_cptr_, d_cnodes_, d_gedges_, d_eocc_, d_triptr_, d_slot_cell_;
+    DevBuf<TriIdx> d_tris_;
+    // setup outputs
+    DevBuf<double> d_A0_, d_A64_, d_W64_, d_P_, d_HW_, d_L_, d_alpha_, d_theta_, d_rhs_, d_bval_;
+    DevBuf<float> d_A32_, d_W32_, d_L32_;
+    DevBuf<int> d_map_, d_mask_;
+    DevBuf<unsigned long long> d_status_;
+    // preconditioner (inverse diagonal of the block-diagonal SPD preconditioner)
+    DevBuf<double> d_dinv64_;
+    DevBuf<float> d_dinv32_;
+    // reductions
+    DevBuf<double> d_partials_;
+    DevBuf<unsigned int> d_counter_;
+    DevBuf<double> d_red_;
+    // Krylov workspaces
+    DevBuf<double> w64_[8];
+    DevBuf<float> w32_[8];
+    DevBuf<double> d_scal_;
+    DevBuf<int> d_flags_;
+    SetupArgs setup_args_{};
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+};
+
+}  // namespace vg
