@@ -143,11 +143,33 @@ def voronoi_polygons(points, r_in, r_out):
     q = np.where(eq.any(axis=1), Ta[np.arange(len(Ta)), eq.argmax(axis=1)], -1)
     if (q < 0).any():
         raise RuntimeError("inconsistent Voronoi ring")
-    # merge coincident circumcentres (zero-length Voronoi edges)
-    tol = 1e-9 * h
-    key = np.round(cc / tol).astype(np.int64)
-    _, vid = np.unique(key, axis=0, return_inverse=True)
-    vid = vid.reshape(-1)
+    # collapse Voronoi edges shorter than 1% of the mean spacing (near-cocircular generators):
+    # the end points are merged globally, so neighbouring cells stay conforming; a merged group
+    # that contains a boundary vertex keeps that vertex's position on the circle
+    vid = np.arange(len(cc))
+    ring_next_t = tid[nxt]
+    d = np.hypot(*(cc[tid] - cc[ring_next_t]).T)
+    short = np.nonzero(d < 1e-2 * h)[0]
+    if len(short):
+        from scipy.sparse import coo_matrix
+        from scipy.sparse.csgraph import connected_components
+        a, b = tid[short], ring_next_t[short]
+        members = np.unique(np.concatenate([a, b]))
+        la, lb = np.searchsorted(members, a), np.searchsorted(members, b)
+        g = coo_matrix((np.ones(len(la)), (la, lb)), shape=(len(members), len(members)))
+        ncomp, lab = connected_components(g, directed=False)
+        root = np.full(ncomp, np.iinfo(np.int64).max)
+        np.minimum.at(root, lab, members)
+        vid[members] = root[lab]
+        onb = (outer | inner)[members]
+        pos = np.zeros((ncomp, 2))
+        cnt = np.zeros(ncomp)
+        np.add.at(pos, lab, cc[members])
+        np.add.at(cnt, lab, 1.0)
+        pos /= cnt[:, None]
+        bsel = np.nonzero(onb)[0]
+        pos[lab[bsel]] = cc[members[bsel]]  # any boundary member (all lie on the circle)
+        cc[members] = pos[lab]
     verts = vid[tid]
     edge_kind = kind[q]  # 0 interior, 1 outer chord, 2 inner chord
     # drop repeated consecutive vertices
