@@ -1,0 +1,333 @@
+"""Benchmark: Darcy solve seconds to relative residual 1e-10 on the 1e6-cell annulus.
+
+Workload (one step = one solve from zero initial guess): annulus 0.3 < r < 1 with exact circular
+arcs, 1e6 seeded Voronoi + 20 Lloyd cells, k = 0, lognormal K (exponential covariance, sigma 2,
+correlation length 0.1), pressure 1 on r = 0.3 and 0 on r = 1, FP32 local operators and inner
+MINRES under FP64 iterative refinement (the headline), the plain FP64 MINRES solve timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--cells C]
+
+Multi-GPU: replicas only (the reference solver does not partition; every configuration fits one
+GPU); each rank solves its own seeded problem, no data-path collective; value = max over ranks.
+``--impl reference`` times the reference CPU algorithm restated in the oracle (element matrices,
+CSR assembly, GMRES(100) + ILU(0), rtol 1e-10) on rank 0 over a bounded sample.
+"""
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "wsl-code_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "Darcy solve s @1e-10 vs FP64 oracle: FP32-refined vs FP64 GPU; HBM GB/s; grad/solve"
+CACHE = os.path.join(ROOT, "wsl-code_b200", "_meshcache")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=1_000_000)
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--cpu-sample-cells", type=int, default=8000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="small run for ncu: few solves, no extras")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def annulus_problem(cells, seed):
+    """Mesh (cached on disk) and log-permeability field of the workload."""
+    import numpy as np
+    from vemgpu import fields, meshgen
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"annulus_{cells}_s{seed}.npz")
+    if os.path.exists(path):
+        z = np.load(path)
+        mesh = {k: z[k] for k in z.files}
+    else:
+        mesh = meshgen.voronoi_mesh(cells, "annulus", seed=seed)
+        mesh = {k: v for k, v in mesh.items() if isinstance(v, np.ndarray)}
+        tmp = path + f".{os.getpid()}.tmp.npz"
+        np.savez(tmp, **mesh)
+        os.replace(tmp, path)
+    theta = fields.gaussian_field(fields.cell_centroids(mesh), sigma=2.0, corr=0.1, seed=seed + 1)
+    return mesh, theta
+
+
+def apply_bytes(g, mesh, fp):
+    """Algorithmic bytes of one apply (k = 0): packed A_E + int32 map + cell id per cell, x read
+    once and y written once (no multiplier, no W at k = 0)."""
+    import numpy as np
+    s = 4 if fp == 32 else 8
+    ne = np.diff(mesh["cell_ptr"]).astype(np.int64)
+    per_cell = s * ne * (ne + 1) // 2 + 4 * ne + 4
+    return int(per_cell.sum() + s * 2 * g.N)
+
+
+class ClockSampler:
+    def __init__(self, path):
+        self.path, self.p = path, None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+            self.f.close()
+
+    def summary(self, device):
+        import statistics
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    t = [c.strip() for c in line.split(",")]
+                    if len(t) >= 9 and t[0] == str(device):
+                        rows.append(t)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_reference(args, threads):
+    """The reference CPU algorithm restated (oracle): assembly + GMRES(100)+ILU(0), one sample solve."""
+    import oracle as O
+    mesh, theta = annulus_problem(args.cpu_sample_cells, args.seed)
+    x, it, tm = O.reference_solve(mesh, k=0, nq=9, ng=9, geom=O.GEOM_ARCS, problem=O.PROB_ANNULUS,
+                                  bc=O.BC_PRESSURE, theta=theta, threads=threads, rtol=1e-10, maxit=200000)
+    return tm["assembly_s"] + tm["solve_s"], it, tm
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    times = []
+    for i in range(args.warmup + args.steps):
+        t, it, tm = cpu_reference(args, threads)
+        if i >= args.warmup:
+            times.append(t)
+    sample = sum(times) / len(times)
+    value = sample * args.cells / args.cpu_sample_cells
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"annulus {args.cells} Voronoi cells, k=0, lognormal K, Dirichlet p=1/0",
+                       "sample_cells": args.cpu_sample_cells},
+            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
+                             "sample": f"reference algorithm restated (oracle): element matrices + CSR assembly "
+                                       f"({threads} threads) + GMRES(100)+ILU(0) rtol 1e-10 (1 thread) on a "
+                                       f"{args.cpu_sample_cells}-cell annulus of the same family, {sample:.2f} s per "
+                                       f"solve, {it} iterations, scaled linearly to {args.cells} cells (a lower "
+                                       f"bound: iterations grow with size)"},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ours(args, rank, world, dist):
+    import numpy as np
+    import torch
+    import vemgpu
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    # rank 0 builds the mesh cache; replicas differ by their permeability seed
+    if rank == 0:
+        annulus_problem(args.cells, args.seed)
+    if dist:
+        dist.barrier()
+    mesh, _ = annulus_problem(args.cells, args.seed)
+    from vemgpu import fields
+    theta = fields.gaussian_field(fields.cell_centroids(mesh), sigma=2.0, corr=0.1, seed=args.seed + 1 + rank)
+    t0 = time.time()
+    g = vemgpu.DarcyGpu(mesh, k=0, nq=9, ng=9, geometry="arcs", problem="annulus", bc="pressure", theta=theta)
+    setup_s = time.time() - t0
+    b = g.rhs()
+    x = g.zeros()
+    if args.profile:
+        # short fixed sequence for profilers: 5 FP32 applies, 5 FP64 applies, 64 inner iterations
+        z = torch.randn(g.N, dtype=torch.float32, device="cuda")
+        y = torch.empty_like(z)
+        for _ in range(5):
+            g.apply(z, out=y)
+        z64, y64 = z.double(), y.double()
+        for _ in range(5):
+            g.apply(z64, out=y64)
+        try:
+            g.solve(b, x, mode="mixed", tol=1e-10, maxit=64, max_outer=1, check_every=64)
+        except vemgpu.VemGpuError:
+            pass
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "done", "cells": g.nc, "dofs": g.N}), flush=True)
+        return
+
+    def solve(mode):
+        return g.solve(b, x, mode=mode, tol=1e-10, inner_tol=1e-5, check_every=64)[1]
+
+    def timed(mode, steps, warmup):
+        for _ in range(warmup):
+            solve(mode)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        infos = []
+        l0 = g.stats()["launches"]
+        e0.record()
+        for _ in range(steps):
+            infos.append(solve(mode))
+        e1.record()
+        torch.cuda.synchronize()
+        launches = g.stats()["launches"] - l0
+        if dist:
+            dist.barrier()
+        ms = e0.elapsed_time(e1) / steps
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), infos, launches
+
+    clk = ClockSampler(os.path.join(tempfile.gettempdir(), f"vg_clocks_{os.getpid()}.csv"))
+    with clk:
+        ms_mixed, info_mixed, launches = timed("mixed", args.steps, args.warmup)
+    clocks = clk.summary(local)
+    x_mixed = x.clone()
+    res = {}
+    if not args.no_fp64 and not args.profile:
+        ms64, info64, _ = timed("fp64", 1, 1)
+        res["fp64"] = dict(solve_s=ms64 * 1e-3, iterations=info64[0]["iterations"], residual=info64[0]["residual"])
+        x64 = x.clone()
+        res["fp64"]["rel_diff_mixed_vs_fp64"] = float(torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64))
+    # per-kernel device times on the same buffers (FP32 apply, FP64 apply) with L2 flushed in between
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    z32 = torch.randn(g.N, dtype=torch.float32, device="cuda")
+    z64 = z32.double()
+
+    def kernel_ms(fn, reps=20):
+        tot = 0.0
+        for _ in range(3):
+            fn()
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / reps
+
+    y32, y64 = torch.empty_like(z32), torch.empty_like(z64)
+    apply32_ms = kernel_ms(lambda: g.apply(z32, out=y32))
+    apply64_ms = kernel_ms(lambda: g.apply(z64, out=y64))
+    b32, b64 = apply_bytes(g, mesh, 32), apply_bytes(g, mesh, 64)
+    peak, peak_kind = peaks()
+    ach32 = b32 / (apply32_ms * 1e-3) / 1e9
+    ach64 = b64 / (apply64_ms * 1e-3) / 1e9
+    # end to end through the host-buffer C ABI call (H2D of b and D2H of x inside)
+    bh = b.cpu().numpy()
+    e2e = []
+    for i in range(1 + args.steps):
+        t = time.perf_counter()
+        xh, info_h = g.solve_host(bh, mode="mixed", tol=1e-10, inner_tol=1e-5, check_every=64)
+        if i:
+            e2e.append(time.perf_counter() - t)
+    e2e_s = sum(e2e) / len(e2e)
+    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_s = float(t.item())
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
+        threads = 1
+        tcpu, it, tm = cpu_reference(args, threads)
+        cpu = {"value": tcpu * args.cells / args.cpu_sample_cells, "unit": "s", "cores": threads, "kind": "port",
+               "sample": f"reference algorithm restated (oracle): element matrices, CSR assembly, GMRES(100)+ILU(0) "
+                         f"rtol 1e-10 on a {args.cpu_sample_cells}-cell annulus of the same family, one core: "
+                         f"{tcpu:.2f} s ({it} iterations), scaled linearly to {args.cells} cells (lower bound)"}
+    if rank != 0:
+        return
+    contrast = float(np.exp(theta.max() - theta.min()))
+    line = {
+        "metric": METRIC, "value": ms_mixed * 1e-3, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"annulus 0.3<r<1, {g.nc} Voronoi+Lloyd cells (exact arcs), k=0, lognormal K "
+                               f"(sigma 2, corr 0.1, K max/min {contrast:.2e}), p=1 inner / 0 outer, FP32 inner "
+                               f"MINRES + FP64 refinement to ||b-Ax||/||b|| <= 1e-10",
+                   "cells": g.nc, "edges": g.ne, "dofs": g.N, "k": 0, "nq": 9, "ng": 9,
+                   "l2": "inputs larger than L2 (per-iteration working set > 126 MB); L2 flushed before each "
+                         "single-kernel timing", "parallelism": f"replicas x{world}"},
+        "iterations": info_mixed[0]["iterations"], "outer": info_mixed[0]["outer"],
+        "residual": info_mixed[0]["residual"], "setup_s": setup_s, "fp64": res.get("fp64"),
+        "kernels": {"apply_fp32_ms": apply32_ms, "apply_fp64_ms": apply64_ms, "apply_fp32_bytes": b32,
+                    "apply_fp64_bytes": b64},
+        "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
+                     "traffic": None, "kernel": "apply_tpl<float,0,NE> (FP32 matrix-free apply, all buckets)",
+                     "peak_kind": peak_kind, "fp64_apply_frac": ach64 / peak},
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * g.N, "d2h_bytes_per_step": 8 * g.N},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    try:
+        ours(args, rank, world, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

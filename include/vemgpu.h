@@ -183,6 +183,10 @@ int vg_errors(vg_handle* h, const double* x, double out[6]);
  * doubles, sign * (index + 1)), 5 rhs (q), 6 Dirichlet load (n). Returns the count in *count. */
 int vg_local(vg_handle* h, int cell, int which, double* out, int* count);
 
+/* Diagnostics (no counterpart in the reference): out[0] = kernels launched by this handle,
+ * out[1] = operator applies, out[2] = Krylov iterations, out[3] = solves, since creation. */
+int vg_stats(const vg_handle* h, long long out[4]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,10 +10,12 @@ template <typename T>
 struct ApplyArgs {
     const T* x;
     T* y;               // flux edge entries must be zero on entry (atomic scatter)
-    const T* A;         // packed A_E, slot-major per bucket
-    const T* W;         // W_E (k >= 1), slot-major per bucket
-    const int* map;     // signed flux dof map, slot-major per bucket
+    const T* A;         // packed A_E, piece layout
+    const T* W;         // W_E (k >= 1), piece layout
+    const int* map;     // signed flux dof map, piece layout
     const int* slot_cell;
+    const Piece* pieces;
+    int npieces, k;
     const T* L;         // multiplier vector per cell (q), when mult
     const int* mask;    // essential-BC mask (N), when constrained
     const int* flags;   // optional: skip when flags[0] != 0
@@ -26,9 +28,10 @@ struct ApplyArgs {
     int total_blocks, block_off;
 };
 
-int apply_blocks(const std::vector<Bucket>& buckets);
+constexpr int APPLY_THREADS = 256;
+int apply_blocks(int npieces);
 
 template <typename T>
-void launch_apply(ApplyArgs<T> a, const std::vector<Bucket>& buckets, int k, cudaStream_t s);
+void launch_apply(ApplyArgs<T> a, cudaStream_t s);
 
 }  // namespace vg

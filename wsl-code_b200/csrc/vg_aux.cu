@@ -8,32 +8,42 @@ namespace {
 
 __device__ __forceinline__ int packed_diag(int i, int n) { return i * n - i * (i - 1) / 2; }
 
+// thread per slot: piece index and lane, false for padding lanes
+__device__ __forceinline__ bool slot_of(const Piece* pieces, int npieces, Piece& P, int& lane) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int pc = int(t / PIECE);
+    lane = int(t % PIECE);
+    if (pc >= npieces) return false;
+    P = pieces[pc];
+    return lane < P.count;
+}
+
 // assembled diagonal of the flux block: d[g] += A_E,ii (at most two addends per edge dof)
-__global__ void k_diag_flux(const double* A, const int* map, Bucket b, double* d) {
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= b.count) return;
-    const long long m = b.count;
-    for (int i = 0; i < b.n; ++i) {
-        int g = map[b.map_off + i * m + j];
-        atomicAdd(d + (g < 0 ? ~g : g), A[b.a_off + (long long)packed_diag(i, b.n) * m + j]);
+__global__ void k_diag_flux(const double* A, const int* map, const Piece* pieces, int npieces, double* d) {
+    Piece P;
+    int lane;
+    if (!slot_of(pieces, npieces, P, lane)) return;
+    for (int i = 0; i < P.n; ++i) {
+        int g = map[P.map_off + i * PIECE + lane];
+        atomicAdd(d + (g < 0 ? ~g : g), A[P.a_off + (long long)packed_diag(i, P.n) * PIECE + lane]);
     }
 }
 
 // pressure diagonal S_rr = sum_i W_ri^2 / d_i over free flux dofs; multiplier contribution
 __global__ void k_diag_finish(const double* W, const int* map, const int* slot_cell, const int* mask, const double* L,
-                              Bucket b, int k, long long nf, double* d, double* contrib) {
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= b.count) return;
-    const long long m = b.count;
-    const int q = (k + 1) * (k + 2) / 2, ed = (k + 1) * b.ne;
-    const int cell = slot_cell[b.slot + j];
+                              const Piece* pieces, int npieces, int k, long long nf, double* d, double* contrib) {
+    Piece P;
+    int lane;
+    if (!slot_of(pieces, npieces, P, lane)) return;
+    const int q = (k + 1) * (k + 2) / 2, ed = (k + 1) * P.ne;
+    const int cell = slot_cell[P.slot + lane];
     double c = 0;
     for (int r = 0; r < q; ++r) {
         double s = 0;
-        for (int i = 0; i < b.n; ++i) {
-            int g = map[b.map_off + i * m + j], idx = g < 0 ? ~g : g;
+        for (int i = 0; i < P.n; ++i) {
+            int g = map[P.map_off + i * PIECE + lane], idx = g < 0 ? ~g : g;
             if (mask && i < ed && mask[idx]) continue;
-            double w = k == 0 ? 1.0 : W[b.w_off + (long long)(r * b.n + i) * m + j];
+            double w = k == 0 ? 1.0 : W[P.w_off + (long long)(r * P.n + i) * PIECE + lane];
             s += w * w / fmax(fabs(d[idx]), 1e-300);
         }
         s = fmax(s, 1e-300);
@@ -75,14 +85,15 @@ __global__ void k_lift(const int* mask, const double* g, const double* y, double
         b[i] = mask[i] ? g[i] : b[i] - y[i];
 }
 
-__global__ void k_rescale(const double* theta, const int* slot_cell, Bucket b, const double* A0, double* A64, float* A32) {
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= b.count) return;
-    const long long m = b.count;
-    double et = exp(-theta[slot_cell[b.slot + j]]);
-    int npk = b.n * (b.n + 1) / 2;
+__global__ void k_rescale(const double* theta, const int* slot_cell, const Piece* pieces, int npieces, const double* A0,
+                          double* A64, float* A32) {
+    Piece P;
+    int lane;
+    if (!slot_of(pieces, npieces, P, lane)) return;
+    double et = exp(-theta[slot_cell[P.slot + lane]]);
+    int npk = P.n * (P.n + 1) / 2;
     for (int e = 0; e < npk; ++e) {
-        long long o = b.a_off + e * m + j;
+        long long o = P.a_off + (long long)e * PIECE + lane;
         double v = et * A0[o];
         A64[o] = v;
         A32[o] = float(v);
@@ -91,26 +102,27 @@ __global__ void k_rescale(const double* theta, const int* slot_cell, Bucket b, c
 
 constexpr int ADJ_MAXN = 5 * MAX_NE + 24;
 
-__global__ void k_contract(const double* A, const int* map, const int* slot_cell, const int* mask, Bucket b, int ed,
-                           const double* x, const double* mu, int constrained, double* g) {
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= b.count) return;
-    const long long m = b.count;
+__global__ void k_contract(const double* A, const int* map, const int* slot_cell, const int* mask, const Piece* pieces,
+                           int npieces, int k, const double* x, const double* mu, int constrained, double* g) {
+    Piece P;
+    int lane;
+    if (!slot_of(pieces, npieces, P, lane)) return;
+    const int ed = (k + 1) * P.ne;
     double u[ADJ_MAXN], w[ADJ_MAXN];
-    for (int i = 0; i < b.n; ++i) {
-        int gi = map[b.map_off + i * m + j], idx = gi < 0 ? ~gi : gi;
+    for (int i = 0; i < P.n; ++i) {
+        int gi = map[P.map_off + i * PIECE + lane], idx = gi < 0 ? ~gi : gi;
         double s = gi < 0 ? -1.0 : 1.0;
         u[i] = s * x[idx];
         w[i] = (constrained && i < ed && mask[idx]) ? 0.0 : s * mu[idx];
     }
     double acc = 0;
     long long e = 0;
-    for (int i = 0; i < b.n; ++i)
-        for (int c = i; c < b.n; ++c) {
-            double a = A[b.a_off + (e++) * m + j];
+    for (int i = 0; i < P.n; ++i)
+        for (int c = i; c < P.n; ++c) {
+            double a = A[P.a_off + (e++) * PIECE + lane];
             acc += c == i ? a * w[i] * u[i] : a * (w[i] * u[c] + w[c] * u[i]);
         }
-    g[slot_cell[b.slot + j]] = acc;
+    g[slot_cell[P.slot + lane]] = acc;
 }
 
 __global__ void k_axpy64(double* x, const double* d, double a, long long n) {
@@ -122,15 +134,15 @@ inline int blocks_for(long long n) { return int((n + 255) / 256); }
 
 }  // namespace
 
-void diag_flux(const double* A, const int* map, const Bucket& b, double* d, cudaStream_t s) {
-    k_diag_flux<<<blocks_for(b.count), 256, 0, s>>>(A, map, b, d);
+void diag_flux(const double* A, const int* map, const Piece* pieces, int npieces, double* d, cudaStream_t s) {
+    k_diag_flux<<<blocks_for((long long)npieces * PIECE), 256, 0, s>>>(A, map, pieces, npieces, d);
     VG_CUDA(cudaGetLastError());
 }
 
-void diag_finish(const double* A, const double* W, const int* map, const int* slot_cell, const int* mask,
-                 const double* L, const Bucket& b, int k, long long nf, double* d, double* contrib, cudaStream_t s) {
-    (void)A;
-    k_diag_finish<<<blocks_for(b.count), 256, 0, s>>>(W, map, slot_cell, mask, L, b, k, nf, d, contrib);
+void diag_finish(const double* W, const int* map, const int* slot_cell, const int* mask, const double* L,
+                 const Piece* pieces, int npieces, int k, long long nf, double* d, double* contrib, cudaStream_t s) {
+    k_diag_finish<<<blocks_for((long long)npieces * PIECE), 256, 0, s>>>(W, map, slot_cell, mask, L, pieces, npieces,
+                                                                         k, nf, d, contrib);
     VG_CUDA(cudaGetLastError());
 }
 
@@ -151,21 +163,17 @@ void lift_rhs(const int* mask, const double* g, const double* y, double* b, long
     VG_CUDA(cudaGetLastError());
 }
 
-void rescale_ops(const double* theta, const int* slot_cell, const Bucket& b, const double* A0, double* A64, float* A32,
-                 cudaStream_t s) {
-    k_rescale<<<blocks_for(b.count), 256, 0, s>>>(theta, slot_cell, b, A0, A64, A32);
+void rescale_ops(const double* theta, const int* slot_cell, const Piece* pieces, int npieces, const double* A0,
+                 double* A64, float* A32, cudaStream_t s) {
+    k_rescale<<<blocks_for((long long)npieces * PIECE), 256, 0, s>>>(theta, slot_cell, pieces, npieces, A0, A64, A32);
     VG_CUDA(cudaGetLastError());
 }
 
-void contract_adjoint(const double* A, const int* map, const int* slot_cell, const int* mask, const Bucket& b,
-                      const double* x, const double* mu, int constrained, double* g, cudaStream_t s) {
-    int ed = b.n;  // edge dofs: all but the interior ones; recomputed from the map owner below
-    (void)ed;
-    // edge dofs are the first (k+1) n_e local dofs; k is recovered from n and n_e:
-    // n = (k+1) n_e + internal(k) is increasing in k
-    int k = 0;
-    while ((k + 1) * b.ne + internal_of(k) != b.n) ++k;
-    k_contract<<<blocks_for(b.count), 256, 0, s>>>(A, map, slot_cell, mask, b, (k + 1) * b.ne, x, mu, constrained, g);
+void contract_adjoint(const double* A, const int* map, const int* slot_cell, const int* mask, const Piece* pieces,
+                      int npieces, int k, const double* x, const double* mu, int constrained, double* g,
+                      cudaStream_t s) {
+    k_contract<<<blocks_for((long long)npieces * PIECE), 256, 0, s>>>(A, map, slot_cell, mask, pieces, npieces, k, x, mu,
+                                                                      constrained, g);
     VG_CUDA(cudaGetLastError());
 }
 

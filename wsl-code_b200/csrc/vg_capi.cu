@@ -209,4 +209,13 @@ int vg_local(vg_handle* h, int cell, int which, double* out, int* count) {
     });
 }
 
+int vg_stats(const vg_handle* h, long long out[4]) {
+    if (!h || !h->s || !out) return VG_EINVAL;
+    out[0] = h->s->n_launch;
+    out[1] = h->s->n_apply;
+    out[2] = h->s->n_iter;
+    out[3] = h->s->n_solve;
+    return VG_OK;
+}
+
 }  // extern "C"

@@ -282,18 +282,32 @@ struct TriIdx {
     uint8_t a, b, c, arc;
 };
 
-// one bucket of cells with the same number of edges; arrays are slot-major inside the bucket:
-// entry e of slot j lives at base + e * count + j
-struct Bucket {
+// Operator layout. Cells (in mesh order, which the generators make a Hilbert order) are cut into
+// chunks of CHUNK cells; inside a chunk the cells are grouped by edge count and every group is
+// split into pieces of at most PIECE cells. One piece = one warp in the apply kernel: its cells
+// share the edge count (warp-uniform control flow) and live in one compact region of the mesh
+// (gathers of x and scatters into y stay local). Per-cell arrays are stored piece-major with the
+// lane innermost: entry e of lane l of a piece lives at off + e * PIECE + l, so every entry load of
+// a warp is one coalesced 128-byte (FP32) or 256-byte (FP64) transaction.
+constexpr int PIECE = 32;
+constexpr int CHUNK = 4096;
+struct Piece {
     int ne;            // edges per cell
     int n;             // local flux dofs
-    int count;         // cells in the bucket
-    long long slot;    // first slot (global slot index)
-    long long a_off;   // packed A entries (n(n+1)/2 per cell)
-    long long w_off;   // W entries (q n per cell, k >= 1)
-    long long map_off; // map entries (n per cell)
-    long long p_off;   // P entries (p n per cell)
-    long long hw_off;  // H^{-1} W entries (q n per cell)
+    int count;         // cells in the piece (<= PIECE); lanes >= count are padding
+    int pad_;
+    long long slot;    // first slot (PIECE per piece); slot = PIECE * piece + lane
+    long long a_off;   // packed A_E, n(n+1)/2 entries per cell
+    long long w_off;   // W_E (k >= 1), q n entries per cell
+    long long map_off; // signed flux dof map, n entries per cell
+    long long p_off;   // projector P, p n entries per cell
+    long long hw_off;  // H^{-1} W, q n entries per cell
+};
+
+// cells with the same edge count (setup and error kernels are launched per class)
+struct CellClass {
+    int ne, n, count;
+    const int* cells;  // device list
 };
 
 }  // namespace vg

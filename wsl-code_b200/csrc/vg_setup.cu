@@ -167,15 +167,18 @@ __device__ static int cell_volume_points(const SetupArgs& a, int cell, const dou
     return npt;
 }
 
-__global__ void setup_kernel(SetupArgs a, Bucket b, SmemLayout L) {
+__global__ void setup_kernel(SetupArgs a, CellClass cls, SmemLayout L) {
     extern __shared__ double sm[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    const int j = blockIdx.x * wpb + wid;
-    if (j >= b.count) return;
+    const int jc = blockIdx.x * wpb + wid;
+    if (jc >= cls.count) return;
     double* S = sm + size_t(wid) * L.per_warp;
-    const int cell = a.slot_cell[b.slot + j];
-    const int ne = b.ne, n = b.n, k = a.k, q = a.q, p = a.p, ng = a.ng, ngr = a.ngrad, ed = (k + 1) * ne;
-    const int m = b.count;
+    const int cell = cls.cells[jc];
+    const int slot = a.cell_slot[cell];
+    const Piece b = a.pieces[slot / PIECE];
+    const int j = slot % PIECE;
+    const int ne = cls.ne, n = cls.n, k = a.k, q = a.q, p = a.p, ng = a.ng, ngr = a.ngrad, ed = (k + 1) * ne;
+    const int m = PIECE;
     const Frame f{a.cx[cell], a.cy[cell], a.diam[cell]};
     const int vb = a.cptr[cell];
     double* V = S + L.vert;
@@ -508,7 +511,7 @@ SmemLayout make_layout(int k, int ne, int nqp, int ng) {
     return L;
 }
 
-void launch_setup(const SetupArgs& a, const Bucket& b, int nqp, cudaStream_t s) {
+void launch_setup(const SetupArgs& a, const CellClass& b, int nqp, cudaStream_t s) {
     SmemLayout L = make_layout(a.k, b.ne, nqp, a.ng);
     size_t per = size_t(L.per_warp) * sizeof(double);
     int wpb = int(std::max<size_t>(1, std::min<size_t>(4, (96u << 10) / per)));
@@ -523,14 +526,17 @@ void launch_setup(const SetupArgs& a, const Bucket& b, int nqp, cudaStream_t s) 
 // Six error figures per cell (MixedGpu::errors, vem/CurvedVEM_Darcy_gpu/src/equation_gpu.cu:387-462):
 // projected flux P u, divergence H^{-1} W u, errors against the built-in exact solution on the
 // computational and the physical domain, and the physical pressure mass. One warp per cell.
-__global__ void error_kernel(SetupArgs a, Bucket b, SmemLayout L, const double* x, double* per_cell) {
+__global__ void error_kernel(SetupArgs a, CellClass cls, SmemLayout L, const double* x, double* per_cell) {
     extern __shared__ double sm[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    const int j = blockIdx.x * wpb + wid;
-    if (j >= b.count) return;
+    const int jc = blockIdx.x * wpb + wid;
+    if (jc >= cls.count) return;
     double* S = sm + size_t(wid) * L.per_warp;
-    const int cell = a.slot_cell[b.slot + j];
-    const int ne = b.ne, n = b.n, k = a.k, q = a.q, p = a.p, m = b.count;
+    const int cell = cls.cells[jc];
+    const int slot = a.cell_slot[cell];
+    const Piece b = a.pieces[slot / PIECE];
+    const int j = slot % PIECE;
+    const int ne = cls.ne, n = cls.n, k = a.k, q = a.q, p = a.p, m = PIECE;
     const Frame f{a.cx[cell], a.cy[cell], a.diam[cell]};
     const int vb = a.cptr[cell];
     double* V = S + L.vert;
@@ -622,7 +628,7 @@ __global__ void error_sum_kernel(const double* per_cell, int nc, double* out) {
     if (t < 6) out[t] = t == 5 ? sh[5][0] : sqrt(fmax(sh[t][0], 0.0));
 }
 
-void launch_errors(const SetupArgs& a, const Bucket& b, int nqp, const double* x, double* per_cell, cudaStream_t s) {
+void launch_errors(const SetupArgs& a, const CellClass& b, int nqp, const double* x, double* per_cell, cudaStream_t s) {
     SmemLayout L = make_layout(a.k, b.ne, nqp, a.ng);
     size_t per = size_t(L.per_warp) * sizeof(double);
     int wpb = int(std::max<size_t>(1, std::min<size_t>(4, (96u << 10) / per)));

@@ -18,7 +18,9 @@ struct SetupArgs {
     const TriIdx* tris;
     const double* arc;  // 3 per global edge (cx, cy, r), r = 0 for straight edges; null unless arcs
     const int* slot_cell;
-    const int* map;     // slot-major signed flux dof map
+    const int* cell_slot;
+    const Piece* pieces;
+    const int* map;     // signed flux dof map, piece layout
     const double* theta;
     int k, q, p, ngrad, internal, nqp, ng, geom, problem, bc, nf;
     double eps;
@@ -47,9 +49,9 @@ struct SmemLayout {
 
 void upload_rules(const std::vector<double>& tri, const std::vector<double>& gl);
 SmemLayout make_layout(int k, int ne, int nqp, int ng);
-void launch_setup(const SetupArgs& a, const Bucket& b, int nqp, cudaStream_t s);
+void launch_setup(const SetupArgs& a, const CellClass& c, int nqp, cudaStream_t s);
 // six error figures per cell into per_cell (6 doubles per cell, cell order), x in reference layout
-void launch_errors(const SetupArgs& a, const Bucket& b, int nqp, const double* x, double* per_cell, cudaStream_t s);
+void launch_errors(const SetupArgs& a, const CellClass& c, int nqp, const double* x, double* per_cell, cudaStream_t s);
 // deterministic sum of per-cell figures -> out[6] (square roots of the five error figures)
 void launch_error_sum(const double* per_cell, int nc, double* out, cudaStream_t s);
 

@@ -11,16 +11,17 @@
 
 namespace vg {
 
-void diag_flux(const double* A, const int* map, const Bucket& b, double* d, cudaStream_t s);
-void diag_finish(const double* A, const double* W, const int* map, const int* slot_cell, const int* mask,
-                 const double* L, const Bucket& b, int k, long long nf, double* d, double* contrib, cudaStream_t s);
+void diag_flux(const double* A, const int* map, const Piece* pieces, int npieces, double* d, cudaStream_t s);
+void diag_finish(const double* W, const int* map, const int* slot_cell, const int* mask, const double* L,
+                 const Piece* pieces, int npieces, int k, long long nf, double* d, double* contrib, cudaStream_t s);
 void diag_invert(double* d, const int* mask, const double* contrib, int nc, long long nf, long long np, int mult,
                  long long N, cudaStream_t s);
 void lift_rhs(const int* mask, const double* g, const double* y, double* b, long long N, cudaStream_t s);
-void rescale_ops(const double* theta, const int* slot_cell, const Bucket& b, const double* A0, double* A64, float* A32,
-                 cudaStream_t s);
-void contract_adjoint(const double* A, const int* map, const int* slot_cell, const int* mask, const Bucket& b,
-                      const double* x, const double* mu, int constrained, double* g, cudaStream_t s);
+void rescale_ops(const double* theta, const int* slot_cell, const Piece* pieces, int npieces, const double* A0,
+                 double* A64, float* A32, cudaStream_t s);
+void contract_adjoint(const double* A, const int* map, const int* slot_cell, const int* mask, const Piece* pieces,
+                      int npieces, int k, const double* x, const double* mu, int constrained, double* g,
+                      cudaStream_t s);
 
 namespace {
 
@@ -241,6 +242,8 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
     d_tris_.upload(tris);
     if (geom_kind == VG_GEOM_ARCS) d_arc_.upload(arcdata);
     d_slot_cell_.upload(slot_cell_);
+    d_cell_slot_.upload(cell_slot_);
+    d_pieces_.upload(pieces_);
     d_map_.upload(map_host_);
     {
         std::vector<int> occ(m.eocc);
@@ -263,59 +266,72 @@ Solver::~Solver() {
 }
 
 void Solver::pack_layout() {
-    // buckets by edge count (ascending), cells in increasing id inside a bucket
-    std::vector<std::vector<int>> byne(MAX_NE + 1);
-    for (int c = 0; c < m.nc; ++c) byne[m.cptr[c + 1] - m.cptr[c]].push_back(c);
-    buckets_.clear();
+    // chunks of CHUNK consecutive cells, grouped by edge count inside a chunk, split into pieces
+    pieces_.clear();
     slot_cell_.clear();
     cell_slot_.assign(m.nc, -1);
-    long long slot = 0;
     a_total_ = w_total_ = map_total_ = p_total_ = hw_total_ = 0;
     maxn = 0;
-    for (int ne = 3; ne <= MAX_NE; ++ne) {
-        if (byne[ne].empty()) continue;
-        Bucket b{};
-        b.ne = ne;
-        b.n = (k + 1) * ne + internal;
-        b.count = int(byne[ne].size());
-        b.slot = slot;
-        b.a_off = a_total_;
-        b.w_off = w_total_;
-        b.map_off = map_total_;
-        b.p_off = p_total_;
-        b.hw_off = hw_total_;
-        long long cnt = b.count;
-        a_total_ += cnt * (b.n * (b.n + 1) / 2);
-        w_total_ += k >= 1 ? cnt * q * b.n : 0;
-        map_total_ += cnt * b.n;
-        p_total_ += cnt * p * b.n;
-        hw_total_ += cnt * q * b.n;
-        maxn = std::max(maxn, b.n);
-        for (int c : byne[ne]) {
-            cell_slot_[c] = int(slot_cell_.size());
-            slot_cell_.push_back(c);
-        }
-        slot += cnt;
-        buckets_.push_back(b);
+    std::vector<std::vector<int>> byne(MAX_NE + 1), classes(MAX_NE + 1);
+    for (int c0 = 0; c0 < m.nc; c0 += CHUNK) {
+        int c1 = std::min(m.nc, c0 + CHUNK);
+        for (auto& v : byne) v.clear();
+        for (int c = c0; c < c1; ++c) byne[m.cptr[c + 1] - m.cptr[c]].push_back(c);
+        for (int ne = 3; ne <= MAX_NE; ++ne)
+            for (size_t s0 = 0; s0 < byne[ne].size(); s0 += PIECE) {
+                Piece P{};
+                P.ne = ne;
+                P.n = (k + 1) * ne + internal;
+                P.count = int(std::min<size_t>(PIECE, byne[ne].size() - s0));
+                P.slot = (long long)pieces_.size() * PIECE;
+                P.a_off = a_total_;
+                P.w_off = w_total_;
+                P.map_off = map_total_;
+                P.p_off = p_total_;
+                P.hw_off = hw_total_;
+                a_total_ += (long long)PIECE * (P.n * (P.n + 1) / 2);
+                w_total_ += k >= 1 ? (long long)PIECE * q * P.n : 0;
+                map_total_ += (long long)PIECE * P.n;
+                p_total_ += (long long)PIECE * p * P.n;
+                hw_total_ += (long long)PIECE * q * P.n;
+                maxn = std::max(maxn, P.n);
+                for (int l = 0; l < PIECE; ++l) {
+                    int c = l < P.count ? byne[ne][s0 + l] : -1;
+                    if (c >= 0) {
+                        cell_slot_[c] = int(slot_cell_.size());
+                        classes[ne].push_back(c);
+                    }
+                    slot_cell_.push_back(c);
+                }
+                pieces_.push_back(P);
+            }
     }
+    classes_.clear();
+    class_cells_.clear();
+    for (int ne = 3; ne <= MAX_NE; ++ne)
+        if (!classes[ne].empty()) {
+            class_cells_.emplace_back();
+            class_cells_.back().upload(classes[ne]);
+            classes_.push_back(CellClass{ne, (k + 1) * ne + internal, int(classes[ne].size()),
+                                         class_cells_.back().data()});
+        }
     // signed flux dof map (vem/CurvedVEM_Darcy_gpu/src/mesh_pack.cpp:209-225): edge moments degree-major,
     // sign -1 on even moments of an interior edge traversed against its (min, max) orientation
     map_host_.assign(map_total_, 0);
-    for (const auto& b : buckets_) {
-        for (int j = 0; j < b.count; ++j) {
-            int c = slot_cell_[b.slot + j];
+    for (const auto& P : pieces_) {
+        for (int j = 0; j < P.count; ++j) {
+            int c = slot_cell_[P.slot + j];
             int base = m.cptr[c];
             for (int r = 0; r <= k; ++r)
-                for (int e = 0; e < b.ne; ++e) {
+                for (int e = 0; e < P.ne; ++e) {
                     int ge = m.gedges[base + e];
                     int g = r * m.ne + ge;
                     bool rev = m.cnodes[base + e] != m.eend[2 * ge];
                     bool neg = m.eocc[ge] == 2 && rev && r % 2 == 0;
-                    map_host_[b.map_off + (long long)(r * b.ne + e) * b.count + j] = neg ? ~g : g;
+                    map_host_[P.map_off + (long long)(r * P.ne + e) * PIECE + j] = neg ? ~g : g;
                 }
             for (int i = 0; i < internal; ++i)
-                map_host_[b.map_off + (long long)((k + 1) * b.ne + i) * b.count + j] =
-                    m.ne * (k + 1) + c * internal + i;
+                map_host_[P.map_off + (long long)((k + 1) * P.ne + i) * PIECE + j] = m.ne * (k + 1) + c * internal + i;
         }
     }
 }
@@ -336,8 +352,8 @@ void Solver::set_theta(const double* theta, bool on_device) {
     else
         VG_CUDA(cudaMemcpy(d_theta_.data(), theta, sizeof(double) * m.nc, cudaMemcpyHostToDevice));
     if (built) {
-        for (const auto& b : buckets_)
-            rescale_ops(d_theta_.data(), d_slot_cell_.data(), b, d_A0_.data(), d_A64_.data(), d_A32_.data(), nullptr);
+        rescale_ops(d_theta_.data(), d_slot_cell_.data(), d_pieces_.data(), int(pieces_.size()), d_A0_.data(),
+                    d_A64_.data(), d_A32_.data(), nullptr);
         make_diagonal(nullptr);
         VG_CUDA(cudaDeviceSynchronize());
     }
@@ -387,6 +403,8 @@ void Solver::build() {
     a.tris = d_tris_.data();
     a.arc = geom_kind == VG_GEOM_ARCS ? d_arc_.data() : nullptr;
     a.slot_cell = d_slot_cell_.data();
+    a.cell_slot = d_cell_slot_.data();
+    a.pieces = d_pieces_.data();
     a.map = d_map_.data();
     a.theta = d_theta_.data();
     a.k = k;
@@ -416,11 +434,11 @@ void Solver::build() {
     a.mask = d_mask_.data();
     a.status = d_status_.data();
     setup_args_ = a;
-    for (const auto& b : buckets_) launch_setup(a, b, nqp, nullptr);
+    for (const auto& c : classes_) launch_setup(a, c, nqp, nullptr);
     VG_CUDA(cudaDeviceSynchronize());
     check_status("setup");
     // workspaces
-    d_partials_.resize(2 * size_t(std::max(apply_blocks(buckets_), VEC_BLOCKS)) + 16);
+    d_partials_.resize(2 * size_t(std::max(apply_blocks(int(pieces_.size())), VEC_BLOCKS)) + 16);
     d_red_.resize(8);
     d_scal_.resize(sizeof(Scalars) / sizeof(double) + 1);
     d_flags_.resize(NFLAGS);
@@ -449,11 +467,10 @@ void Solver::make_diagonal(cudaStream_t s) {
     // (the diagonal of vem/CurvedVEM_Darcy_gpu/src/equation_gpu.cu:282-315 with |.| of the Schur part)
     DevBuf<double> contrib(m.nc);
     d_dinv64_.zero(s);
-    for (const auto& b : buckets_) diag_flux(d_A64_.data(), d_map_.data(), b, d_dinv64_.data(), s);
-    for (const auto& b : buckets_)
-        diag_finish(d_A64_.data(), d_W64_.data(), d_map_.data(), d_slot_cell_.data(),
-                    bc == VG_BC_FLUX ? d_mask_.data() : nullptr, d_L_.data(), b, k, nf, d_dinv64_.data(),
-                    contrib.data(), s);
+    const int np_ = int(pieces_.size());
+    diag_flux(d_A64_.data(), d_map_.data(), d_pieces_.data(), np_, d_dinv64_.data(), s);
+    diag_finish(d_W64_.data(), d_map_.data(), d_slot_cell_.data(), bc == VG_BC_FLUX ? d_mask_.data() : nullptr,
+                d_L_.data(), d_pieces_.data(), np_, k, nf, d_dinv64_.data(), contrib.data(), s);
     diag_invert(d_dinv64_.data(), bc == VG_BC_FLUX ? d_mask_.data() : nullptr, contrib.data(), m.nc, nf, np,
                 bc == VG_BC_FLUX, N, s);
     to_float_plain(d_dinv64_.data(), d_dinv32_.data(), N, s);
@@ -468,6 +485,9 @@ void Solver::apply64(const double* x, double* y, bool constrained, double psign,
     a.W = d_W64_.data();
     a.map = d_map_.data();
     a.slot_cell = d_slot_cell_.data();
+    a.pieces = d_pieces_.data();
+    a.npieces = int(pieces_.size());
+    a.k = k;
     a.L = d_L_.data();
     a.mask = d_mask_.data();
     a.flags = nullptr;
@@ -479,7 +499,9 @@ void Solver::apply64(const double* x, double* y, bool constrained, double psign,
     a.partials = d_partials_.data();
     a.counter = d_counter_.data();
     a.red = quad;
-    launch_apply(a, buckets_, k, s);
+    launch_apply(a, s);
+    n_launch += 1;
+    ++n_apply;
 }
 
 void Solver::apply32(const float* x, float* y, bool constrained, float psign, cudaStream_t s, double* quad) {
@@ -490,6 +512,9 @@ void Solver::apply32(const float* x, float* y, bool constrained, float psign, cu
     a.W = d_W32_.data();
     a.map = d_map_.data();
     a.slot_cell = d_slot_cell_.data();
+    a.pieces = d_pieces_.data();
+    a.npieces = int(pieces_.size());
+    a.k = k;
     a.L = d_L32_.data();
     a.mask = d_mask_.data();
     a.flags = nullptr;
@@ -501,7 +526,9 @@ void Solver::apply32(const float* x, float* y, bool constrained, float psign, cu
     a.partials = d_partials_.data();
     a.counter = d_counter_.data();
     a.red = quad;
-    launch_apply(a, buckets_, k, s);
+    launch_apply(a, s);
+    n_launch += 1;
+    ++n_apply;
 }
 
 void Solver::rhs(double* b, cudaStream_t s) {
@@ -532,6 +559,9 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
                 a.W = d_W32_.data();
                 a.map = d_map_.data();
                 a.slot_cell = d_slot_cell_.data();
+                a.pieces = d_pieces_.data();
+                a.npieces = int(pieces_.size());
+                a.k = k;
                 a.L = d_L32_.data();
                 a.mask = d_mask_.data();
                 a.flags = flags;
@@ -543,7 +573,9 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
                 a.partials = d_partials_.data();
                 a.counter = d_counter_.data();
                 a.red = &sc->delta;
-                launch_apply(a, buckets_, k, s);
+                launch_apply(a, s);
+                n_launch += 3;
+                ++n_apply;
                 minres_update<float>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s);
                 minres_step<float>(v, N, sc, flags, s);
                 std::swap(v.v_cur, v.v_old);
@@ -572,6 +604,9 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
                 a.W = d_W64_.data();
                 a.map = d_map_.data();
                 a.slot_cell = d_slot_cell_.data();
+                a.pieces = d_pieces_.data();
+                a.npieces = int(pieces_.size());
+                a.k = k;
                 a.L = d_L_.data();
                 a.mask = d_mask_.data();
                 a.flags = flags;
@@ -583,7 +618,9 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
                 a.partials = d_partials_.data();
                 a.counter = d_counter_.data();
                 a.red = &sc->delta;
-                launch_apply(a, buckets_, k, s);
+                launch_apply(a, s);
+                n_launch += 3;
+                ++n_apply;
                 minres_update<double>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s);
                 minres_step<double>(v, N, sc, flags, s);
                 std::swap(v.v_cur, v.v_old);
@@ -597,6 +634,8 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
         }
     }
     iters = h_flags[2];
+    n_iter += iters;
+    n_launch += 1;  // init
 }
 
 void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_info& info, cudaStream_t s) {
@@ -609,12 +648,15 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
     // symmetric form: pressure / multiplier rows negated
     DevBuf<double> bs(N), r(N), y(N), d(N);
     flip_pressure(b, bs.data(), nf, N, s);
+    n_launch += 1;
+    ++n_solve;
     if (!o.nonzero_guess) VG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
     double h_red[2] = {0, 0};
     auto true_residual = [&]() {
         y.zero(s);
         apply64(x, y.data(), cons, -1.0, s);
         residual64(bs.data(), y.data(), r.data(), N, d_red_.data(), d_partials_.data(), d_counter_.data(), s);
+        n_launch += 1;
         VG_CUDA(cudaMemcpyAsync(h_red, d_red_.data(), sizeof(h_red), cudaMemcpyDeviceToHost, s));
         VG_CUDA(cudaStreamSynchronize(s));
         double nb = std::sqrt(h_red[1]);
@@ -632,6 +674,7 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
             minres(false, r.data(), d.data(), std::min(0.5, 0.1 * o.tol * nb / rn), o.maxit - total, o.check_every, it, s);
             total += it;
             axpy64(x, d.data(), 1.0, s);
+            n_launch += 1;
             rel = true_residual();
         }
     } else {
@@ -639,6 +682,7 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
         for (outer = 0; outer < o.max_outer && rel > o.tol && total < o.maxit; ++outer) {
             double rn = rel * nb;
             to_float(r.data(), r32.data(), 1.0 / rn, N, s);
+            n_launch += 2;
             int it = 0;
             minres(true, r32.data(), d32.data(), o.inner_tol, o.maxit - total, o.check_every, it, s);
             total += it;
@@ -674,16 +718,15 @@ void Solver::adjoint(const double* x, const double* dJdx, double* g, const vg_so
     oo.nonzero_guess = 0;
     solve(rhs.data(), mu.data(), oo, info, s);
     // dJ/dtheta_E = -lambda^T (dK/dtheta_E) x = mu_u,E^T A_E(theta) x_u,E  (dA_E/dtheta_E = -A_E)
-    for (const auto& b : buckets_)
-        contract_adjoint(d_A64_.data(), d_map_.data(), d_slot_cell_.data(), d_mask_.data(), b, x, mu.data(),
-                         bc == VG_BC_FLUX, g, s);
+    contract_adjoint(d_A64_.data(), d_map_.data(), d_slot_cell_.data(), d_mask_.data(), d_pieces_.data(),
+                     int(pieces_.size()), k, x, mu.data(), bc == VG_BC_FLUX, g, s);
     VG_CUDA(cudaStreamSynchronize(s));
 }
 
 void Solver::errors(const double* x, double out[6], cudaStream_t s) {
     if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_errors");
     DevBuf<double> per(6 * size_t(m.nc)), sum(6);
-    for (const auto& b : buckets_) launch_errors(setup_args_, b, nq, x, per.data(), s);
+    for (const auto& c : classes_) launch_errors(setup_args_, c, nq, x, per.data(), s);
     launch_error_sum(per.data(), m.nc, sum.data(), s);
     VG_CUDA(cudaMemcpyAsync(out, sum.data(), 6 * sizeof(double), cudaMemcpyDeviceToHost, s));
     VG_CUDA(cudaStreamSynchronize(s));
@@ -693,11 +736,8 @@ int Solver::local(int cell, int which, double* out) {
     if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_local");
     if (cell < 0 || cell >= m.nc) throw Error(VG_EINVAL, "cell out of range");
     int slot = cell_slot_[cell];
-    const Bucket* bk = nullptr;
-    for (const auto& b : buckets_)
-        if (slot >= b.slot && slot < b.slot + b.count) bk = &b;
-    const Bucket& b = *bk;
-    long long j = slot - b.slot, mcount = b.count;
+    const Piece& b = pieces_[slot / PIECE];
+    long long j = slot % PIECE, mcount = PIECE;
     int n = b.n;
     auto strided = [&](const double* base, long long off, int cnt, std::vector<double>& v) {
         v.resize(cnt);

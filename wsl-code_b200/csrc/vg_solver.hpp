@@ -56,6 +56,7 @@ public:
     int k, nq, ng, q, p, ngrad, internal, nf, np, N, maxn;
     int problem = VG_PROBLEM_SINCOS, bc = VG_BC_FLUX;
     bool built = false;
+    long long n_launch = 0, n_apply = 0, n_iter = 0, n_solve = 0;
     std::string error;
 
     HostMesh m;
@@ -64,8 +65,6 @@ public:
 
 private:
     void pack_layout();
-    void setup_kernels();
-    void rescale(cudaStream_t s);
     void make_diagonal(cudaStream_t s);
     void check_status(const char* where);
     void axpy64(double* x, const double* d, double a, cudaStream_t s);
@@ -73,16 +72,19 @@ private:
                 cudaStream_t s);
 
     int device_ = 0;
-    std::vector<Bucket> buckets_;
-    std::vector<int> slot_cell_;   // slot -> cell
+    std::vector<Piece> pieces_;
+    std::vector<int> slot_cell_;   // slot -> cell (-1 on padding lanes)
     std::vector<int> cell_slot_;   // cell -> slot
-    std::vector<int> map_host_;    // slot-major signed map (~g for negative orientation)
+    std::vector<int> map_host_;    // signed flux dof map, piece layout (~g for negative orientation)
+    std::vector<CellClass> classes_;
+    std::vector<DevBuf<int>> class_cells_;
     std::vector<double> theta_;
     long long a_total_ = 0, w_total_ = 0, map_total_ = 0, p_total_ = 0, hw_total_ = 0;
 
     // mesh / geometry on the device
     DevBuf<double> d_xy_, d_cx_, d_cy_, d_diam_, d_arc_;
-    DevBuf<int> d_cptr_, d_cnodes_, d_gedges_, d_eocc_, d_triptr_, d_slot_cell_;
+    DevBuf<int> d_cptr_, d_cnodes_, d_gedges_, d_eocc_, d_triptr_, d_slot_cell_, d_cell_slot_;
+    DevBuf<Piece> d_pieces_;
     DevBuf<TriIdx> d_tris_;
     // setup outputs
     DevBuf<double> d_A0_, d_A64_, d_W64_, d_P_, d_HW_, d_L_, d_alpha_, d_theta_, d_rhs_, d_bval_;

@@ -91,7 +91,10 @@ class DarcyGpu:
 
     def close(self):
         if getattr(self, "h", None):
-            L.lib().vg_destroy(self.h)
+            try:
+                L.lib().vg_destroy(self.h)
+            except Exception:
+                pass
             self.h = None
 
     def __del__(self):
@@ -168,6 +171,11 @@ class DarcyGpu:
         out = (ctypes.c_double * 6)()
         L.check(L.lib().vg_errors(self.h, x.data_ptr(), out), self.h)
         return dict(zip(("scalar_comp", "flux_comp", "scalar_phys", "flux_phys", "div_phys", "mass"), list(out)))
+
+    def stats(self):
+        out = (ctypes.c_longlong * 4)()
+        L.check(L.lib().vg_stats(self.h, out), self.h)
+        return dict(launches=out[0], applies=out[1], iterations=out[2], solves=out[3])
 
     def local(self, cell, which):
         names = dict(A=0, W=1, P=2, alpha=3, map=4, rhs=5, dload=6)
