@@ -1,0 +1,461 @@
+// Smoothed-aggregation AMG: host setup, device V-cycle (see vg_amg.hpp).
+//
+// Setup (host, once per operator): strength of connection |a_ij| >= theta sqrt(a_ii a_jj);
+// three-phase greedy aggregation in row order (rows are cells in Hilbert order, so aggregates are
+// compact); tentative prolongator = aggregate indicator; prolongator smoothed by one damped Jacobi
+// step P = (I - omega D^{-1} A) P_tent with omega = 4 / (3 rho(D^{-1} A)); Galerkin coarse operator
+// R A P with R = P^T; stop at <= 512 rows and invert the coarsest matrix densely.
+// Cycle (device): symmetric V(1,1) cycle with damped Jacobi (same omega) — a fixed symmetric
+// positive definite operator, as MINRES requires of its preconditioner.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "vg_amg.hpp"
+
+namespace vg {
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// host sparse kernels
+// ---------------------------------------------------------------------------------------------
+HostCsr transpose(const HostCsr& A) {
+    HostCsr T;
+    T.n = A.m;
+    T.m = A.n;
+    T.ptr.assign(T.n + 1, 0);
+    for (int c : A.col) T.ptr[c + 1]++;
+    for (int i = 0; i < T.n; ++i) T.ptr[i + 1] += T.ptr[i];
+    T.col.resize(A.col.size());
+    T.val.resize(A.val.size());
+    std::vector<int> fill(T.ptr.begin(), T.ptr.end() - 1);
+    for (int i = 0; i < A.n; ++i)
+        for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j) {
+            int d = fill[A.col[j]]++;
+            T.col[d] = i;
+            T.val[d] = A.val[j];
+        }
+    return T;
+}
+
+HostCsr spgemm(const HostCsr& A, const HostCsr& B) {
+    HostCsr C;
+    C.n = A.n;
+    C.m = B.m;
+    C.ptr.assign(C.n + 1, 0);
+    std::vector<int> mark(B.m, -1), cols;
+    std::vector<double> acc(B.m, 0.0);
+    for (int i = 0; i < A.n; ++i) {
+        cols.clear();
+        for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j) {
+            int k = A.col[j];
+            double a = A.val[j];
+            for (int t = B.ptr[k]; t < B.ptr[k + 1]; ++t) {
+                int c = B.col[t];
+                if (mark[c] != i) {
+                    mark[c] = i;
+                    acc[c] = 0.0;
+                    cols.push_back(c);
+                }
+                acc[c] += a * B.val[t];
+            }
+        }
+        std::sort(cols.begin(), cols.end());
+        for (int c : cols) {
+            C.col.push_back(c);
+            C.val.push_back(acc[c]);
+        }
+        C.ptr[i + 1] = int(C.col.size());
+    }
+    return C;
+}
+
+double diag_of(const HostCsr& A, int i) {
+    for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j)
+        if (A.col[j] == i) return A.val[j];
+    return 0.0;
+}
+
+// largest eigenvalue of D^{-1} A by power iteration (seeded start vector)
+double rho_dinv_a(const HostCsr& A, const std::vector<double>& dinv) {
+    int n = A.n;
+    std::vector<double> v(n), w(n);
+    unsigned s = 12345u;
+    for (int i = 0; i < n; ++i) {
+        s = s * 1103515245u + 12345u;
+        v[i] = 0.5 + (s >> 16) / 65536.0;
+    }
+    double lam = 1.0;
+    for (int it = 0; it < 20; ++it) {
+        double nv = 0;
+        for (int i = 0; i < n; ++i) {
+            double a = 0;
+            for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j) a += A.val[j] * v[A.col[j]];
+            w[i] = dinv[i] * a;
+            nv += w[i] * w[i];
+        }
+        nv = std::sqrt(nv);
+        if (!(nv > 0)) break;
+        double dv = 0;
+        for (int i = 0; i < n; ++i) dv += w[i] * v[i];
+        double vv = 0;
+        for (int i = 0; i < n; ++i) vv += v[i] * v[i];
+        lam = dv / vv;
+        for (int i = 0; i < n; ++i) v[i] = w[i] / nv;
+    }
+    return std::max(lam, 1e-300);
+}
+
+// three-phase greedy aggregation on the strong-connection graph
+std::vector<int> aggregate(const HostCsr& A, double theta, int& nagg) {
+    int n = A.n;
+    std::vector<double> d(n);
+    for (int i = 0; i < n; ++i) d[i] = std::fabs(diag_of(A, i));
+    auto strong = [&](int i, int j, double a) {
+        return j != i && std::fabs(a) >= theta * std::sqrt(d[i] * d[j]);
+    };
+    std::vector<int> agg(n, -1);
+    nagg = 0;
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0) continue;
+        bool free = true;
+        for (int j = A.ptr[i]; j < A.ptr[i + 1] && free; ++j)
+            if (strong(i, A.col[j], A.val[j]) && agg[A.col[j]] >= 0) free = false;
+        if (!free) continue;
+        agg[i] = nagg;
+        for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j)
+            if (strong(i, A.col[j], A.val[j])) agg[A.col[j]] = nagg;
+        ++nagg;
+    }
+    std::vector<int> first(agg);
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0) continue;
+        double best = -1;
+        int bj = -1;
+        for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j) {
+            int c = A.col[j];
+            if (strong(i, c, A.val[j]) && first[c] >= 0 && std::fabs(A.val[j]) > best) {
+                best = std::fabs(A.val[j]);
+                bj = c;
+            }
+        }
+        if (bj >= 0) agg[i] = first[bj];
+    }
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0) continue;
+        agg[i] = nagg;
+        for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j)
+            if (strong(i, A.col[j], A.val[j]) && agg[A.col[j]] < 0) agg[A.col[j]] = nagg;
+        ++nagg;
+    }
+    return agg;
+}
+
+// P = (I - omega D^{-1} A) P_tent
+HostCsr smoothed_prolongator(const HostCsr& A, const std::vector<int>& agg, int nagg, const std::vector<double>& dinv,
+                             double omega) {
+    HostCsr P;
+    P.n = A.n;
+    P.m = nagg;
+    P.ptr.assign(A.n + 1, 0);
+    std::vector<int> mark(nagg, -1), cols;
+    std::vector<double> acc(nagg, 0.0);
+    for (int i = 0; i < A.n; ++i) {
+        cols.clear();
+        auto add = [&](int c, double v) {
+            if (mark[c] != i) {
+                mark[c] = i;
+                acc[c] = 0.0;
+                cols.push_back(c);
+            }
+            acc[c] += v;
+        };
+        add(agg[i], 1.0);
+        for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j) add(agg[A.col[j]], -omega * dinv[i] * A.val[j]);
+        std::sort(cols.begin(), cols.end());
+        for (int c : cols)
+            if (acc[c] != 0.0) {
+                P.col.push_back(c);
+                P.val.push_back(acc[c]);
+            }
+        P.ptr[i + 1] = int(P.col.size());
+    }
+    return P;
+}
+
+// dense symmetric inverse by Gauss-Jordan with partial pivoting; a tiny diagonal shift keeps a
+// semi-definite coarsest matrix (pure flux boundary: constants in the kernel) invertible
+std::vector<double> dense_inverse(const HostCsr& A) {
+    int n = A.n;
+    std::vector<double> a(size_t(n) * n, 0.0), inv(size_t(n) * n, 0.0);
+    double tr = 0;
+    for (int i = 0; i < n; ++i)
+        for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j) {
+            a[size_t(i) * n + A.col[j]] += A.val[j];
+            if (A.col[j] == i) tr += A.val[j];
+        }
+    for (int i = 0; i < n; ++i) {
+        a[size_t(i) * n + i] += 1e-12 * tr / n;
+        inv[size_t(i) * n + i] = 1.0;
+    }
+    for (int k = 0; k < n; ++k) {
+        int piv = k;
+        for (int i = k + 1; i < n; ++i)
+            if (std::fabs(a[size_t(i) * n + k]) > std::fabs(a[size_t(piv) * n + k])) piv = i;
+        if (piv != k)
+            for (int j = 0; j < n; ++j) {
+                std::swap(a[size_t(k) * n + j], a[size_t(piv) * n + j]);
+                std::swap(inv[size_t(k) * n + j], inv[size_t(piv) * n + j]);
+            }
+        double dk = a[size_t(k) * n + k];
+        if (!(std::fabs(dk) > 0)) throw Error(VG_ESINGULAR, "singular coarsest multigrid matrix");
+        for (int j = 0; j < n; ++j) {
+            a[size_t(k) * n + j] /= dk;
+            inv[size_t(k) * n + j] /= dk;
+        }
+        for (int i = 0; i < n; ++i)
+            if (i != k) {
+                double f = a[size_t(i) * n + k];
+                if (f == 0.0) continue;
+                for (int j = 0; j < n; ++j) {
+                    a[size_t(i) * n + j] -= f * a[size_t(k) * n + j];
+                    inv[size_t(i) * n + j] -= f * inv[size_t(k) * n + j];
+                }
+            }
+    }
+    // symmetrise (the exact inverse is symmetric)
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) {
+            double v = 0.5 * (inv[size_t(i) * n + j] + inv[size_t(j) * n + i]);
+            inv[size_t(i) * n + j] = inv[size_t(j) * n + i] = v;
+        }
+    return inv;
+}
+
+// ---------------------------------------------------------------------------------------------
+// device kernels (SELL-32, one thread per row)
+// ---------------------------------------------------------------------------------------------
+constexpr int TPB = 256;
+
+template <typename T>
+__device__ __forceinline__ T sell_row(const DevSell<T>& M, int r, const T* x) {
+    int s = r >> 5, l = r & 31;
+    long long o = M.soff[s] + l;
+    int w = M.width[s];
+    T acc = T(0);
+    for (int k = 0; k < w; ++k) acc += M.val[o + 32LL * k] * x[M.col[o + 32LL * k]];
+    return acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_jacobi0(int n, const T* dinv, T omega, const T* b, T* x) {
+    int i = blockIdx.x * TPB + threadIdx.x;
+    if (i < n) x[i] = omega * dinv[i] * b[i];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_residual(DevSell<T> A, const T* b, const T* x, T* r) {
+    int i = blockIdx.x * TPB + threadIdx.x;
+    if (i < A.n) r[i] = b[i] - sell_row(A, i, x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_spmv(DevSell<T> M, const T* x, T* y) {
+    int i = blockIdx.x * TPB + threadIdx.x;
+    if (i < M.n) y[i] = sell_row(M, i, x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_prolong_add(DevSell<T> P, const T* xc, T* x) {
+    int i = blockIdx.x * TPB + threadIdx.x;
+    if (i < P.n) x[i] += sell_row(P, i, xc);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_smooth(DevSell<T> A, const T* dinv, T omega, const T* b, const T* x, T* xo) {
+    int i = blockIdx.x * TPB + threadIdx.x;
+    if (i < A.n) xo[i] = x[i] + omega * dinv[i] * (b[i] - sell_row(A, i, x));
+}
+
+// coarsest level: z = Ainv b, one warp per row
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_dense(int n, const T* Ainv, const T* b, T* z) {
+    int row = (blockIdx.x * TPB + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= n) return;
+    T acc = T(0);
+    for (int j = lane; j < n; j += 32) acc += Ainv[(long long)row * n + j] * b[j];
+    for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) z[row] = acc;
+}
+
+inline int blocks(int n) { return (n + TPB - 1) / TPB; }
+
+}  // namespace
+
+long long Amg::nnz() const {
+    long long t = 0;
+    for (const auto& L : levels_) t += (long long)L.A.col.size();
+    return t;
+}
+
+void Amg::setup(const HostCsr& S0) {
+    levels_.clear();
+    HostCsr A = S0;
+    const double theta = 0.08;
+    while (true) {
+        Level L;
+        L.n = A.n;
+        L.dinv.resize(A.n);
+        for (int i = 0; i < A.n; ++i) {
+            double d = diag_of(A, i);
+            L.dinv[i] = d != 0.0 ? 1.0 / d : 0.0;
+        }
+        auto to_sell = [](const HostCsr& M, Sell& S) {
+            S.n = M.n;
+            S.nslices = (M.n + 31) / 32;
+            S.soff.assign(S.nslices + 1, 0);
+            S.width.assign(S.nslices, 0);
+            for (int s = 0; s < S.nslices; ++s) {
+                int w = 0;
+                for (int r = s * 32; r < std::min(M.n, s * 32 + 32); ++r) w = std::max(w, M.ptr[r + 1] - M.ptr[r]);
+                S.width[s] = w;
+                S.soff[s + 1] = S.soff[s] + 32LL * w;
+            }
+            S.col.assign(S.soff[S.nslices], 0);
+            S.val.assign(S.soff[S.nslices], 0.0);
+            for (int s = 0; s < S.nslices; ++s)
+                for (int l = 0; l < 32; ++l) {
+                    int r = s * 32 + l;
+                    for (int k = 0; k < S.width[s]; ++k) {
+                        long long o = S.soff[s] + 32LL * k + l;
+                        if (r < M.n && k < M.ptr[r + 1] - M.ptr[r]) {
+                            S.col[o] = M.col[M.ptr[r] + k];
+                            S.val[o] = M.val[M.ptr[r] + k];
+                        } else {
+                            // padding reads column 0, which every matrix has (P and R are rectangular:
+                            // the row index is not a valid column)
+                            S.col[o] = 0;
+                            S.val[o] = 0.0;
+                        }
+                    }
+                }
+        };
+        to_sell(A, L.A);
+        if (A.n <= 512 || levels_.size() >= 16) {
+            levels_.push_back(std::move(L));
+            break;
+        }
+        int nagg = 0;
+        std::vector<int> agg = aggregate(A, theta, nagg);
+        if (nagg >= A.n || nagg == 0) {  // no coarsening possible
+            levels_.push_back(std::move(L));
+            break;
+        }
+        L.omega = 4.0 / (3.0 * rho_dinv_a(A, L.dinv));
+        HostCsr P = smoothed_prolongator(A, agg, nagg, L.dinv, L.omega);
+        HostCsr R = transpose(P);
+        HostCsr Ac = spgemm(R, spgemm(A, P));
+        L.nc = nagg;
+        to_sell(P, L.P);
+        to_sell(R, L.R);
+        levels_.push_back(std::move(L));
+        A = std::move(Ac);
+    }
+    // coarsest level: dense inverse (bounded size; otherwise the caller keeps its diagonal preconditioner)
+    if (A.n > 4096) {
+        levels_.clear();
+        throw Error(VG_EINVAL, "multigrid coarsening stalled at " + std::to_string(A.n) + " rows");
+    }
+    std::vector<double> inv = dense_inverse(A);
+    ncoarse_ = A.n;
+    dinvc64_.upload(inv);
+    std::vector<float> inv32(inv.begin(), inv.end());
+    dinvc32_.upload(inv32);
+    // uploads
+    for (auto& L : levels_) {
+        auto up = [](const Sell& S, DevBuf<long long>& so, DevBuf<int>& w, DevBuf<int>& c, DevBuf<double>& v64,
+                     DevBuf<float>& v32) {
+            if (S.n == 0) return;
+            so.upload(S.soff);
+            w.upload(S.width);
+            c.upload(S.col);
+            v64.upload(S.val);
+            std::vector<float> f(S.val.begin(), S.val.end());
+            v32.upload(f);
+        };
+        up(L.A, L.dA_soff, L.dA_w, L.dA_col, L.dA_v64, L.dA_v32);
+        up(L.P, L.dP_soff, L.dP_w, L.dP_col, L.dP_v64, L.dP_v32);
+        up(L.R, L.dR_soff, L.dR_w, L.dR_col, L.dR_v64, L.dR_v32);
+        L.dinv64.upload(L.dinv);
+        std::vector<float> f(L.dinv.begin(), L.dinv.end());
+        L.dinv32.upload(f);
+        for (auto* b : {&L.x64, &L.b64, &L.r64, &L.t64}) b->resize(L.n);
+        for (auto* b : {&L.x32, &L.b32, &L.r32, &L.t32}) b->resize(L.n);
+    }
+}
+
+template <typename T>
+DevSell<T> Amg::view(const Level& L, int which) const {
+    DevSell<T> v;
+    const Sell& S = which == 0 ? L.A : which == 1 ? L.P : L.R;
+    v.n = S.n;
+    v.nslices = S.nslices;
+    const DevBuf<long long>& so = which == 0 ? L.dA_soff : which == 1 ? L.dP_soff : L.dR_soff;
+    const DevBuf<int>& w = which == 0 ? L.dA_w : which == 1 ? L.dP_w : L.dR_w;
+    const DevBuf<int>& c = which == 0 ? L.dA_col : which == 1 ? L.dP_col : L.dR_col;
+    v.soff = so.data();
+    v.width = w.data();
+    v.col = c.data();
+    if constexpr (sizeof(T) == 8)
+        v.val = reinterpret_cast<const T*>((which == 0 ? L.dA_v64 : which == 1 ? L.dP_v64 : L.dR_v64).data());
+    else
+        v.val = reinterpret_cast<const T*>((which == 0 ? L.dA_v32 : which == 1 ? L.dP_v32 : L.dR_v32).data());
+    return v;
+}
+
+template <typename T>
+void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
+    Level& L = levels_[l];
+    auto buf = [&](DevBuf<double>& d64, DevBuf<float>& d32) -> T* {
+        if constexpr (sizeof(T) == 8)
+            return reinterpret_cast<T*>(d64.data());
+        else
+            return reinterpret_cast<T*>(d32.data());
+    };
+    const T* dinv = buf(L.dinv64, L.dinv32);
+    if (l == int(levels_.size()) - 1) {
+        const T* inv = sizeof(T) == 8 ? reinterpret_cast<const T*>(dinvc64_.data())
+                                      : reinterpret_cast<const T*>(dinvc32_.data());
+        k_dense<T><<<(ncoarse_ * 32 + TPB - 1) / TPB, TPB, 0, s>>>(ncoarse_, inv, b, z);
+        ++launches;
+        return;
+    }
+    Level& C = levels_[l + 1];
+    T* t = buf(L.t64, L.t32);
+    T* r = buf(L.r64, L.r32);
+    T* bc = buf(C.b64, C.b32);
+    T* xc = buf(C.x64, C.x32);
+    const T om = T(L.omega);
+    DevSell<T> A = view<T>(L, 0), P = view<T>(L, 1), R = view<T>(L, 2);
+    k_jacobi0<T><<<blocks(L.n), TPB, 0, s>>>(L.n, dinv, om, b, t);
+    k_residual<T><<<blocks(L.n), TPB, 0, s>>>(A, b, t, r);
+    k_spmv<T><<<blocks(C.n), TPB, 0, s>>>(R, r, bc);
+    launches += 3;
+    cycle<T>(l + 1, bc, xc, s);
+    k_prolong_add<T><<<blocks(L.n), TPB, 0, s>>>(P, xc, t);
+    k_smooth<T><<<blocks(L.n), TPB, 0, s>>>(A, dinv, om, b, t, z);
+    launches += 2;
+}
+
+void Amg::vcycle(const double* b, double* z, cudaStream_t s) {
+    cycle<double>(0, b, z, s);
+    VG_CUDA(cudaGetLastError());
+}
+
+void Amg::vcycle(const float* b, float* z, cudaStream_t s) {
+    cycle<float>(0, b, z, s);
+    VG_CUDA(cudaGetLastError());
+}
+
+}  // namespace vg

@@ -1,0 +1,74 @@
+// Smoothed-aggregation algebraic multigrid for the pressure Schur block of the k = 0 saddle point
+// system, S = W diag(A)^{-1} W^T (a cell-graph Laplacian with weights 1/diag(A) on the edges).
+//
+// The reference preconditions with a PETSc ILU(0) on the CPU or, matrix-free, with the diagonal
+// |rate M| + sum W^2/d (vem/CurvedVEM_Darcy_gpu/src/krylov.cu:99-117, src/equation_gpu.cu:282-315),
+// which its own notes call weak for large meshes. Here the pressure block of the SPD block-diagonal
+// MINRES preconditioner is one symmetric V-cycle on S (Jacobi pre- and post-smoothing with the same
+// weight, exact coarsest solve), built on the host once per operator and applied on the device.
+#pragma once
+#include <vector>
+
+#include "vg_common.cuh"
+
+namespace vg {
+
+struct HostCsr {
+    int n = 0, m = 0;  // rows, columns
+    std::vector<int> ptr, col;
+    std::vector<double> val;
+};
+
+// sliced ELL with slice height 32: entry k of row r lives at soff[r / 32] + k * 32 + r % 32,
+// padding entries have col = 0 and val = 0
+template <typename T>
+struct DevSell {
+    int n = 0, nslices = 0;
+    const long long* soff = nullptr;
+    const int* width = nullptr;
+    const int* col = nullptr;
+    const T* val = nullptr;
+};
+
+class Amg {
+public:
+    // build the hierarchy of S (host CSR, symmetric positive definite or semi-definite)
+    void setup(const HostCsr& S);
+    bool ready() const { return !levels_.empty(); }
+    int levels() const { return int(levels_.size()); }
+    long long nnz() const;
+    // z = V-cycle(b) on the device (b, z of length n0); FP64 or FP32 copy of the hierarchy
+    void vcycle(const double* b, double* z, cudaStream_t s);
+    void vcycle(const float* b, float* z, cudaStream_t s);
+    long long launches = 0;
+
+private:
+    struct Sell {
+        int n = 0, nslices = 0;
+        std::vector<long long> soff;
+        std::vector<int> width, col;
+        std::vector<double> val;
+    };
+    struct Level {
+        int n = 0, nc = 0;
+        double omega = 0;
+        Sell A, P, R;  // P: n x nc, R = P^T: nc x n (absent on the coarsest level)
+        std::vector<double> dinv;
+        // device
+        DevBuf<long long> dA_soff, dP_soff, dR_soff;
+        DevBuf<int> dA_w, dA_col, dP_w, dP_col, dR_w, dR_col;
+        DevBuf<double> dA_v64, dP_v64, dR_v64, dinv64, x64, b64, r64, t64;
+        DevBuf<float> dA_v32, dP_v32, dR_v32, dinv32, x32, b32, r32, t32;
+    };
+    template <typename T>
+    void cycle(int l, const T* b, T* z, cudaStream_t s);
+    template <typename T>
+    DevSell<T> view(const Level& L, int which) const;
+
+    std::vector<Level> levels_;
+    int ncoarse_ = 0;
+    DevBuf<double> dinvc64_;  // dense inverse of the coarsest matrix
+    DevBuf<float> dinvc32_;
+};
+
+}  // namespace vg

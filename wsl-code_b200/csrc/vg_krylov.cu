@@ -66,40 +66,83 @@ __device__ void grid_reduce(double (&v)[NV], double* partials, unsigned* counter
     }
 }
 
+__device__ void init_scalars(Scalars* sc, int* flags, double g2, double tol) {
+    double g = sqrt(fmax(g2, 0.0));
+    sc->gam = g;
+    sc->gam_prev = 1.0;
+    sc->c_prev = 1.0;
+    sc->c = 1.0;
+    sc->s_prev = 0.0;
+    sc->s = 0.0;
+    sc->eta = g;
+    sc->eta0 = g;
+    sc->tol = tol;
+    flags[0] = (g > 0 && isfinite(g)) ? 0 : 1;
+    flags[1] = 0;
+    flags[2] = 0;
+}
+
+// Givens rotation and residual estimate once gamma_{j+1}^2 is known
+__device__ void update_scalars(Scalars* sc, int* flags, double gn2) {
+    const double g = sc->gam, dl = sc->delta / (g * g);
+    double gn = sqrt(fmax(gn2, 0.0));
+    double c = sc->c, cp = sc->c_prev, s = sc->s, sp = sc->s_prev, eta = sc->eta;
+    double a0 = c * dl - cp * s * g;
+    double a1 = sqrt(a0 * a0 + gn * gn);
+    double a2 = s * dl + cp * c * g;
+    double a3 = sp * g;
+    bool ok = a1 > 0 && isfinite(a1);
+    double cn = ok ? a0 / a1 : 1.0, sn = ok ? gn / a1 : 0.0;
+    sc->a1 = ok ? a1 : 1.0;
+    sc->a2 = a2;
+    sc->a3 = a3;
+    sc->zscale = 1.0 / g;
+    sc->xcoef = ok ? cn * eta : 0.0;
+    sc->eta = -sn * eta;
+    sc->c_prev = c;
+    sc->c = cn;
+    sc->s_prev = s;
+    sc->s = sn;
+    sc->gam_prev = g;
+    sc->gam = gn;
+    flags[1] = ok ? 1 : 0;
+    flags[2] += 1;
+    if (!ok || !(gn > 0) || fabs(sc->eta) <= sc->tol * sc->eta0) flags[0] = 1;
+}
+
+// entries in [plo, phi) (the pressure block when it is preconditioned by multigrid) are left to
+// the V-cycle: z is not written there and the dot product is finished by k_finish
 template <typename T>
 __global__ void __launch_bounds__(VEC_THREADS) k_init(const T* r, MinresVecs<T> v, long long n, Scalars* sc,
-                                                      int* flags, double tol, double* partials, unsigned* counter) {
+                                                      int* flags, double tol, double* partials, unsigned* counter,
+                                                      long long plo, long long phi) {
     double acc[1] = {0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        T ri = r[i], zi = v.dinv[i] * ri;
+        T ri = r[i];
         v.v_cur[i] = ri;
         v.v_old[i] = T(0);
-        v.z_cur[i] = zi;
         v.w_cur[i] = T(0);
         v.w_old[i] = T(0);
         v.y[i] = T(0);
-        acc[0] += double(zi) * double(ri);
+        if (i < plo || i >= phi) {
+            T zi = v.dinv[i] * ri;
+            v.z_cur[i] = zi;
+            acc[0] += double(zi) * double(ri);
+        }
     }
+    const bool split = phi > plo;
     grid_reduce<1>(acc, partials, counter, [&](double* tot) {
-        double g = sqrt(fmax(tot[0], 0.0));
-        sc->gam = g;
-        sc->gam_prev = 1.0;
-        sc->c_prev = 1.0;
-        sc->c = 1.0;
-        sc->s_prev = 0.0;
-        sc->s = 0.0;
-        sc->eta = g;
-        sc->eta0 = g;
-        sc->tol = tol;
-        flags[0] = (g > 0 && isfinite(g)) ? 0 : 1;
-        flags[1] = 0;
-        flags[2] = 0;
+        if (split)
+            sc->dot = tot[0];
+        else
+            init_scalars(sc, flags, tot[0], tol);
     });
 }
 
 template <typename T>
 __global__ void __launch_bounds__(VEC_THREADS) k_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags,
-                                                        double* partials, unsigned* counter) {
+                                                        double* partials, unsigned* counter, long long plo,
+                                                        long long phi) {
     if (flags[0]) {
         if (blockIdx.x == 0 && threadIdx.x == 0) flags[1] = 0;
         return;
@@ -109,36 +152,39 @@ __global__ void __launch_bounds__(VEC_THREADS) k_update(MinresVecs<T> v, long lo
     double acc[1] = {0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         T vn = v.y[i] * f1 - f2 * v.v_cur[i] - f3 * v.v_old[i];
-        T zn = v.dinv[i] * vn;
         v.v_old[i] = vn;
-        v.z_new[i] = zn;
         v.y[i] = T(0);
-        acc[0] += double(zn) * double(vn);
+        if (i < plo || i >= phi) {
+            T zn = v.dinv[i] * vn;
+            v.z_new[i] = zn;
+            acc[0] += double(zn) * double(vn);
+        }
     }
+    const bool split = phi > plo;
     grid_reduce<1>(acc, partials, counter, [&](double* tot) {
-        double gn = sqrt(fmax(tot[0], 0.0));
-        double c = sc->c, cp = sc->c_prev, s = sc->s, sp = sc->s_prev, eta = sc->eta;
-        double a0 = c * dl - cp * s * g;
-        double a1 = sqrt(a0 * a0 + gn * gn);
-        double a2 = s * dl + cp * c * g;
-        double a3 = sp * g;
-        bool ok = a1 > 0 && isfinite(a1);
-        double cn = ok ? a0 / a1 : 1.0, sn = ok ? gn / a1 : 0.0;
-        sc->a1 = ok ? a1 : 1.0;
-        sc->a2 = a2;
-        sc->a3 = a3;
-        sc->zscale = 1.0 / g;
-        sc->xcoef = ok ? cn * eta : 0.0;
-        sc->eta = -sn * eta;
-        sc->c_prev = c;
-        sc->c = cn;
-        sc->s_prev = s;
-        sc->s = sn;
-        sc->gam_prev = g;
-        sc->gam = gn;
-        flags[1] = ok ? 1 : 0;
-        flags[2] += 1;
-        if (!ok || !(gn > 0) || fabs(sc->eta) <= sc->tol * sc->eta0) flags[0] = 1;
+        if (split)
+            sc->dot = tot[0];
+        else
+            update_scalars(sc, flags, tot[0]);
+    });
+}
+
+// pressure part of gamma^2 = z . v after the V-cycle, then the scalar update (init or iteration)
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_finish(const T* z, const T* vv, long long plo, long long phi,
+                                                        Scalars* sc, int* flags, double* partials, unsigned* counter,
+                                                        int init, double tol) {
+    if (!init && flags[0]) return;
+    double acc[1] = {0};
+    for (long long i = plo + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < phi;
+         i += (long long)gridDim.x * blockDim.x)
+        acc[0] += double(z[i]) * double(vv[i]);
+    grid_reduce<1>(acc, partials, counter, [&](double* tot) {
+        double g2 = tot[0] + sc->dot;
+        if (init)
+            init_scalars(sc, flags, g2, tol);
+        else
+            update_scalars(sc, flags, g2);
     });
 }
 
@@ -192,15 +238,22 @@ __global__ void k_to_float_plain(const double* in, float* out, long long n) {
 
 template <typename T>
 void minres_init(const T* r, MinresVecs<T> v, long long n, Scalars* sc, int* flags, double tol, double* partials,
-                 unsigned* counter, cudaStream_t s) {
-    k_init<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(r, v, n, sc, flags, tol, partials, counter);
+                 unsigned* counter, cudaStream_t s, long long plo, long long phi) {
+    k_init<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(r, v, n, sc, flags, tol, partials, counter, plo, phi);
     VG_CUDA(cudaGetLastError());
 }
 
 template <typename T>
 void minres_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags, double* partials, unsigned* counter,
-                   cudaStream_t s) {
-    k_update<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(v, n, sc, flags, partials, counter);
+                   cudaStream_t s, long long plo, long long phi) {
+    k_update<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(v, n, sc, flags, partials, counter, plo, phi);
+    VG_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void minres_finish(const T* z, const T* v, long long plo, long long phi, Scalars* sc, int* flags, double* partials,
+                   unsigned* counter, int init, double tol, cudaStream_t s) {
+    k_finish<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(z, v, plo, phi, sc, flags, partials, counter, init, tol);
     VG_CUDA(cudaGetLastError());
 }
 
@@ -211,11 +264,17 @@ void minres_step(MinresVecs<T> v, long long n, Scalars* sc, int* flags, cudaStre
 }
 
 template void minres_init<double>(const double*, MinresVecs<double>, long long, Scalars*, int*, double, double*,
-                                  unsigned*, cudaStream_t);
+                                  unsigned*, cudaStream_t, long long, long long);
 template void minres_init<float>(const float*, MinresVecs<float>, long long, Scalars*, int*, double, double*,
-                                 unsigned*, cudaStream_t);
-template void minres_update<double>(MinresVecs<double>, long long, Scalars*, int*, double*, unsigned*, cudaStream_t);
-template void minres_update<float>(MinresVecs<float>, long long, Scalars*, int*, double*, unsigned*, cudaStream_t);
+                                 unsigned*, cudaStream_t, long long, long long);
+template void minres_update<double>(MinresVecs<double>, long long, Scalars*, int*, double*, unsigned*, cudaStream_t,
+                                    long long, long long);
+template void minres_update<float>(MinresVecs<float>, long long, Scalars*, int*, double*, unsigned*, cudaStream_t,
+                                   long long, long long);
+template void minres_finish<double>(const double*, const double*, long long, long long, Scalars*, int*, double*,
+                                    unsigned*, int, double, cudaStream_t);
+template void minres_finish<float>(const float*, const float*, long long, long long, Scalars*, int*, double*,
+                                   unsigned*, int, double, cudaStream_t);
 template void minres_step<double>(MinresVecs<double>, long long, Scalars*, int*, cudaStream_t);
 template void minres_step<float>(MinresVecs<float>, long long, Scalars*, int*, cudaStream_t);
 

@@ -28,11 +28,15 @@ struct MinresVecs {
 // z = dinv .* r ; v_cur = r ; v_old = w_cur = w_old = y = 0 ; gamma_1 = sqrt(z.r)
 template <typename T>
 void minres_init(const T* r, MinresVecs<T> v, long long n, Scalars* sc, int* flags, double tol, double* partials,
-                 unsigned* counter, cudaStream_t s);
+                 unsigned* counter, cudaStream_t s, long long plo = 0, long long phi = 0);
 // v_new = y/g - (d/g) v_cur - (g/g_prev) v_old (into v_old), z_new = dinv .* v_new, y = 0, scalars
 template <typename T>
 void minres_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags, double* partials, unsigned* counter,
-                   cudaStream_t s);
+                   cudaStream_t s, long long plo = 0, long long phi = 0);
+// gamma^2 over [plo, phi) + the partial of init / update, then the scalar recurrences
+template <typename T>
+void minres_finish(const T* z, const T* v, long long plo, long long phi, Scalars* sc, int* flags, double* partials,
+                   unsigned* counter, int init, double tol, cudaStream_t s);
 // w_new = (z_cur/g - a3 w_old - a2 w_cur)/a1 (into w_old), x += xcoef w_new
 template <typename T>
 void minres_step(MinresVecs<T> v, long long n, Scalars* sc, int* flags, cudaStream_t s);

@@ -1,5 +1,6 @@
 // vemgpu Solver: host orchestration of the device setup, apply, Krylov solve, adjoint and errors.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <unordered_map>
@@ -475,6 +476,61 @@ void Solver::make_diagonal(cudaStream_t s) {
                 bc == VG_BC_FLUX, N, s);
     to_float_plain(d_dinv64_.data(), d_dinv32_.data(), N, s);
     VG_CUDA(cudaStreamSynchronize(s));
+    use_amg = false;
+    if (k == 0 && bc == VG_BC_PRESSURE) build_amg();
+}
+
+// pressure Schur block S = W diag(A)^{-1} W^T of the k = 0 system (cell graph: S_EE = sum over the
+// edges of E of 1/d_e, S_EF = -1/d_e across the shared edge e) and its multigrid hierarchy
+void Solver::build_amg() {
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<double> dinv(nf);
+    VG_CUDA(cudaMemcpy(dinv.data(), d_dinv64_.data(), sizeof(double) * nf, cudaMemcpyDeviceToHost));
+    std::vector<int> ec(2 * size_t(m.ne), -1);
+    for (int c = 0; c < m.nc; ++c)
+        for (int j = m.cptr[c]; j < m.cptr[c + 1]; ++j) {
+            int e = m.gedges[j];
+            if (ec[2 * e] < 0)
+                ec[2 * e] = c;
+            else
+                ec[2 * e + 1] = c;
+        }
+    HostCsr S;
+    S.n = S.m = m.nc;
+    S.ptr.assign(m.nc + 1, 0);
+    std::vector<std::pair<int, double>> row;
+    for (int c = 0; c < m.nc; ++c) {
+        row.clear();
+        double diag = 0;
+        for (int j = m.cptr[c]; j < m.cptr[c + 1]; ++j) {
+            int e = m.gedges[j];
+            double d = dinv[e];
+            diag += d;
+            int o = ec[2 * e] == c ? ec[2 * e + 1] : ec[2 * e];
+            if (o >= 0) row.push_back({o, -d});
+        }
+        row.push_back({c, diag});
+        std::sort(row.begin(), row.end());
+        for (size_t i = 0; i < row.size(); ++i) {
+            if (i > 0 && row[i].first == row[i - 1].first) {
+                S.val.back() += row[i].second;
+                continue;
+            }
+            S.col.push_back(row[i].first);
+            S.val.push_back(row[i].second);
+        }
+        S.ptr[c + 1] = int(S.col.size());
+    }
+    try {
+        amg_.setup(S);
+    } catch (const Error&) {
+        use_amg = false;  // diagonal preconditioner on the device
+        amg_levels = 0;
+        return;
+    }
+    amg_levels = amg_.levels();
+    use_amg = true;
+    amg_setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 void Solver::apply64(const double* x, double* y, bool constrained, double psign, cudaStream_t s, double* quad) {
@@ -547,7 +603,13 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
                             w32_[4].data(), w32_[5].data(), w32_[6].data(), static_cast<float*>(x),
                             d_dinv32_.data()};
         VG_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * N, s));
-        minres_init<float>(static_cast<const float*>(r), v, N, sc, flags, tol, d_partials_.data(), d_counter_.data(), s);
+        const long long plo = use_amg ? nf : 0, phi = use_amg ? nf + np : 0;
+        minres_init<float>(static_cast<const float*>(r), v, N, sc, flags, tol, d_partials_.data(), d_counter_.data(), s,
+                           plo, phi);
+        if (use_amg) {
+            amg_.vcycle(v.v_cur + nf, v.z_cur + nf, s);
+            minres_finish<float>(v.z_cur, v.v_cur, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(), 1, tol, s);
+        }
         int done = 0;
         while (done < maxit) {
             int batch = std::min(check_every, maxit - done);
@@ -576,7 +638,13 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
                 launch_apply(a, s);
                 n_launch += 3;
                 ++n_apply;
-                minres_update<float>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s);
+                minres_update<float>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s, plo, phi);
+                if (use_amg) {
+                    amg_.vcycle(v.v_old + nf, v.z_new + nf, s);
+                    minres_finish<float>(v.z_new, v.v_old, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(),
+                                         0, tol, s);
+                    n_launch += 1;
+                }
                 minres_step<float>(v, N, sc, flags, s);
                 std::swap(v.v_cur, v.v_old);
                 std::swap(v.z_cur, v.z_new);
@@ -592,7 +660,14 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
                              w64_[4].data(), w64_[5].data(), w64_[6].data(), static_cast<double*>(x),
                              d_dinv64_.data()};
         VG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
-        minres_init<double>(static_cast<const double*>(r), v, N, sc, flags, tol, d_partials_.data(), d_counter_.data(), s);
+        const long long plo = use_amg ? nf : 0, phi = use_amg ? nf + np : 0;
+        minres_init<double>(static_cast<const double*>(r), v, N, sc, flags, tol, d_partials_.data(), d_counter_.data(),
+                            s, plo, phi);
+        if (use_amg) {
+            amg_.vcycle(v.v_cur + nf, v.z_cur + nf, s);
+            minres_finish<double>(v.z_cur, v.v_cur, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(), 1, tol,
+                                  s);
+        }
         int done = 0;
         while (done < maxit) {
             int batch = std::min(check_every, maxit - done);
@@ -621,7 +696,13 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
                 launch_apply(a, s);
                 n_launch += 3;
                 ++n_apply;
-                minres_update<double>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s);
+                minres_update<double>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s, plo, phi);
+                if (use_amg) {
+                    amg_.vcycle(v.v_old + nf, v.z_new + nf, s);
+                    minres_finish<double>(v.z_new, v.v_old, plo, phi, sc, flags, d_partials_.data(),
+                                          d_counter_.data(), 0, tol, s);
+                    n_launch += 1;
+                }
                 minres_step<double>(v, N, sc, flags, s);
                 std::swap(v.v_cur, v.v_old);
                 std::swap(v.z_cur, v.z_new);
@@ -635,7 +716,8 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
     }
     iters = h_flags[2];
     n_iter += iters;
-    n_launch += 1;  // init
+    n_launch += 1 + amg_.launches;  // init + multigrid cycles
+    amg_.launches = 0;
 }
 
 void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_info& info, cudaStream_t s) {

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "vg_common.cuh"
+#include "vg_amg.hpp"
 #include "vg_setup.cuh"
 
 namespace vg {
@@ -57,6 +58,9 @@ public:
     int problem = VG_PROBLEM_SINCOS, bc = VG_BC_FLUX;
     bool built = false;
     long long n_launch = 0, n_apply = 0, n_iter = 0, n_solve = 0;
+    bool use_amg = false;
+    int amg_levels = 0;
+    double amg_setup_s = 0;
     std::string error;
 
     HostMesh m;
@@ -66,6 +70,7 @@ public:
 private:
     void pack_layout();
     void make_diagonal(cudaStream_t s);
+    void build_amg();
     void check_status(const char* where);
     void axpy64(double* x, const double* d, double a, cudaStream_t s);
     void minres(bool fp32, const void* b, void* x, double tol, int maxit, int check_every, int& iters,
@@ -104,6 +109,7 @@ private:
     DevBuf<double> d_scal_;
     DevBuf<int> d_flags_;
     SetupArgs setup_args_{};
+    Amg amg_;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
 };
 
