@@ -28,6 +28,7 @@ for p in (os.path.join(ROOT, "wsl-code_b200"), os.path.join(ROOT, "oracle")):
 
 METRIC = "Darcy solve s @1e-10 vs FP64 oracle: FP32-refined vs FP64 GPU; HBM GB/s; grad/solve"
 CACHE = os.path.join(ROOT, "wsl-code_b200", "_meshcache")
+INNER_TOL = 1e-6  # FP32 inner MINRES: relative reduction per refinement step
 
 
 def parse():
@@ -41,7 +42,8 @@ def parse():
     ap.add_argument("--cpu-sample-cells", type=int, default=8000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--profile", action="store_true", help="small run for ncu: few solves, no extras")
+    ap.add_argument("--profile", action="store_true", help="short fixed run for profilers (applies + 2 solves)")
+    ap.add_argument("--eager", action="store_true", help="with --profile: host-driven Krylov batches, no graph")
     return ap.parse_args()
 
 
@@ -181,7 +183,7 @@ def ours(args, rank, world, dist):
     b = g.rhs()
     x = g.zeros()
     if args.profile:
-        # short fixed sequence for profilers: 5 FP32 applies, 5 FP64 applies, 64 inner iterations
+        # fixed sequence for profilers: 5 FP32 applies, 5 FP64 applies, one FP64 and one mixed solve
         z = torch.randn(g.N, dtype=torch.float32, device="cuda")
         y = torch.empty_like(z)
         for _ in range(5):
@@ -189,16 +191,15 @@ def ours(args, rank, world, dist):
         z64, y64 = z.double(), y.double()
         for _ in range(5):
             g.apply(z64, out=y64)
-        try:
-            g.solve(b, x, mode="mixed", tol=1e-10, maxit=64, max_outer=1, check_every=64)
-        except vemgpu.VemGpuError:
-            pass
+        ce = 16 if args.eager else 0
+        g.solve(b, x, mode="fp64", tol=1e-10, check_every=ce)
+        g.solve(b, x, mode="mixed", tol=1e-10, inner_tol=INNER_TOL, check_every=ce)
         torch.cuda.synchronize()
         print(json.dumps({"profile": "done", "cells": g.nc, "dofs": g.N}), flush=True)
         return
 
     def solve(mode):
-        return g.solve(b, x, mode=mode, tol=1e-10, inner_tol=1e-5, check_every=64)[1]
+        return g.solve(b, x, mode=mode, tol=1e-10, inner_tol=INNER_TOL)[1]
 
     def timed(mode, steps, warmup):
         for _ in range(warmup):
@@ -265,7 +266,7 @@ def ours(args, rank, world, dist):
     e2e = []
     for i in range(1 + args.steps):
         t = time.perf_counter()
-        xh, info_h = g.solve_host(bh, mode="mixed", tol=1e-10, inner_tol=1e-5, check_every=64)
+        xh, info_h = g.solve_host(bh, mode="mixed", tol=1e-10, inner_tol=INNER_TOL)
         if i:
             e2e.append(time.perf_counter() - t)
     e2e_s = sum(e2e) / len(e2e)

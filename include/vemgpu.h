@@ -93,7 +93,9 @@ typedef struct vg_solve_opts {
     int maxit;           /* cap on total inner iterations                                      */
     double inner_tol;    /* MIXED: relative reduction asked of each FP32 inner solve           */
     int max_outer;       /* MIXED: cap on refinement steps                                     */
-    int check_every;     /* iterations between host convergence checks (one graph launch)      */
+    int check_every;     /* 0: the whole Krylov loop is one CUDA graph (device-side while node,
+                            iteration cap on the device); > 0: host-driven batches of this many
+                            iterations, every kernel a plain launch (for profilers)            */
     int nonzero_guess;   /* 1: x holds the initial guess on entry                              */
 } vg_solve_opts;
 

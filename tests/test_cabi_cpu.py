@@ -103,4 +103,4 @@ def test_no_device_is_reported(L):
 def test_default_options(L):
     o = L.VgSolveOpts()
     L.lib().vg_default_solve_opts(ctypes.byref(o))
-    assert o.mode == L.SOLVE_FP64 and o.tol == 1e-10 and o.check_every > 0
+    assert o.mode == L.SOLVE_FP64 and o.tol == 1e-10 and o.check_every == 0 and 0 < o.inner_tol < 1

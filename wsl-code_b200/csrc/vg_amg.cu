@@ -254,6 +254,24 @@ __global__ void __launch_bounds__(TPB) k_jacobi0(int n, const T* dinv, T omega, 
     if (i < n) x[i] = omega * dinv[i] * b[i];
 }
 
+// pre-smoothing from zero fused with the residual: t = omega D^{-1} b, r = b - A t
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_jacobi0_residual(DevSell<T> A, const T* dinv, T omega, const T* b, T* t,
+                                                          T* r) {
+    int i = blockIdx.x * TPB + threadIdx.x;
+    if (i >= A.n) return;
+    int s = i >> 5, l = i & 31;
+    long long o = A.soff[s] + l;
+    int w = A.width[s];
+    T acc = T(0);
+    for (int k = 0; k < w; ++k) {
+        int c = A.col[o + 32LL * k];
+        acc += A.val[o + 32LL * k] * (omega * dinv[c] * b[c]);
+    }
+    t[i] = omega * dinv[i] * b[i];
+    r[i] = b[i] - acc;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_residual(DevSell<T> A, const T* b, const T* x, T* r) {
     int i = blockIdx.x * TPB + threadIdx.x;
@@ -278,6 +296,68 @@ __global__ void __launch_bounds__(TPB) k_smooth(DevSell<T> A, const T* dinv, T o
     if (i < A.n) xo[i] = x[i] + omega * dinv[i] * (b[i] - sell_row(A, i, x));
 }
 
+// ---- CSR, one group of G lanes per row
+template <int G, typename T>
+__device__ __forceinline__ T csr_row(const DevCsr<T>& M, int r, const T* x, int gl) {
+    T acc = T(0);
+    for (int j = M.ptr[r] + gl; j < M.ptr[r + 1]; j += G) acc += M.val[j] * x[M.col[j]];
+#pragma unroll
+    for (int off = G / 2; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off, G);
+    return acc;  // valid in lane gl == 0 of the group
+}
+
+template <int G, typename T>
+__device__ __forceinline__ T csr_row_jac(const DevCsr<T>& M, int r, const T* dinv, T omega, const T* b, int gl) {
+    T acc = T(0);
+    for (int j = M.ptr[r] + gl; j < M.ptr[r + 1]; j += G) {
+        int c = M.col[j];
+        acc += M.val[j] * (omega * dinv[c] * b[c]);
+    }
+#pragma unroll
+    for (int off = G / 2; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off, G);
+    return acc;
+}
+
+// op: 0 y = M x; 1 x += M xc (prolong); 2 smooth xo = x + omega dinv (b - M x); 3 jacobi0 + residual
+template <int G, typename T>
+__global__ void __launch_bounds__(TPB) k_csr(int op, DevCsr<T> M, const T* dinv, T omega, const T* b, const T* x,
+                                             T* y, T* r) {
+    int t = blockIdx.x * TPB + threadIdx.x;
+    int row = t / G, gl = t % G;
+    bool ok = row < M.n;
+    int rr = ok ? row : M.n - 1;  // whole groups stay converged for the shuffles
+    T v;
+    if (op == 3)
+        v = csr_row_jac<G>(M, rr, dinv, omega, b, ok ? gl : G);
+    else
+        v = csr_row<G>(M, rr, x, ok ? gl : G);
+    if (!ok || gl != 0) return;
+    if (op == 0)
+        y[row] = v;
+    else if (op == 1)
+        y[row] += v;
+    else if (op == 2)
+        y[row] = x[row] + omega * dinv[row] * (b[row] - v);
+    else {
+        y[row] = omega * dinv[row] * b[row];
+        r[row] = b[row] - v;
+    }
+}
+
+template <typename T>
+void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, const T* x, T* y, T* r,
+                cudaStream_t s) {
+    if (M.n <= 0) return;
+    long long threads = (long long)M.n * M.group;
+    int blocks = int((threads + TPB - 1) / TPB);
+    switch (M.group) {
+    case 4: k_csr<4, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
+    case 8: k_csr<8, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
+    case 16: k_csr<16, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
+    default: k_csr<32, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
+    }
+}
+
 // coarsest level: z = Ainv b, one warp per row
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_dense(int n, const T* Ainv, const T* b, T* z) {
@@ -295,7 +375,7 @@ inline int blocks(int n) { return (n + TPB - 1) / TPB; }
 
 long long Amg::nnz() const {
     long long t = 0;
-    for (const auto& L : levels_) t += (long long)L.A.col.size();
+    for (const auto& L : levels_) t += (long long)(L.A.csr ? L.A.ccol.size() : L.A.col.size());
     return t;
 }
 
@@ -313,6 +393,16 @@ void Amg::setup(const HostCsr& S0) {
         }
         auto to_sell = [](const HostCsr& M, Sell& S) {
             S.n = M.n;
+            double avg = M.n ? double(M.col.size()) / M.n : 0.0;
+            if (avg > 10.0) {
+                S.csr = true;
+                S.group = avg > 24 ? 32 : avg > 12 ? 16 : 8;
+                S.cptr = M.ptr;
+                S.ccol = M.col;
+                S.cval = M.val;
+                S.nslices = 0;
+                return;
+            }
             S.nslices = (M.n + 31) / 32;
             S.soff.assign(S.nslices + 1, 0);
             S.width.assign(S.nslices, 0);
@@ -376,7 +466,7 @@ void Amg::setup(const HostCsr& S0) {
     for (auto& L : levels_) {
         auto up = [](const Sell& S, DevBuf<long long>& so, DevBuf<int>& w, DevBuf<int>& c, DevBuf<double>& v64,
                      DevBuf<float>& v32) {
-            if (S.n == 0) return;
+            if (S.n == 0 || S.csr) return;
             so.upload(S.soff);
             w.upload(S.width);
             c.upload(S.col);
@@ -387,6 +477,17 @@ void Amg::setup(const HostCsr& S0) {
         up(L.A, L.dA_soff, L.dA_w, L.dA_col, L.dA_v64, L.dA_v32);
         up(L.P, L.dP_soff, L.dP_w, L.dP_col, L.dP_v64, L.dP_v32);
         up(L.R, L.dR_soff, L.dR_w, L.dR_col, L.dR_v64, L.dR_v32);
+        auto upc = [](const Sell& S, DevBuf<int>& p, DevBuf<int>& c, DevBuf<double>& v64, DevBuf<float>& v32) {
+            if (S.n == 0 || !S.csr) return;
+            p.upload(S.cptr);
+            c.upload(S.ccol);
+            v64.upload(S.cval);
+            std::vector<float> f(S.cval.begin(), S.cval.end());
+            v32.upload(f);
+        };
+        upc(L.A, L.cA_ptr, L.cA_col, L.cA_v64, L.cA_v32);
+        upc(L.P, L.cP_ptr, L.cP_col, L.cP_v64, L.cP_v32);
+        upc(L.R, L.cR_ptr, L.cR_col, L.cR_v64, L.cR_v32);
         L.dinv64.upload(L.dinv);
         std::vector<float> f(L.dinv.begin(), L.dinv.end());
         L.dinv32.upload(f);
@@ -415,6 +516,21 @@ DevSell<T> Amg::view(const Level& L, int which) const {
 }
 
 template <typename T>
+DevCsr<T> Amg::cview(const Level& L, int which) const {
+    DevCsr<T> v;
+    const Sell& S = which == 0 ? L.A : which == 1 ? L.P : L.R;
+    v.n = S.n;
+    v.group = S.group;
+    v.ptr = (which == 0 ? L.cA_ptr : which == 1 ? L.cP_ptr : L.cR_ptr).data();
+    v.col = (which == 0 ? L.cA_col : which == 1 ? L.cP_col : L.cR_col).data();
+    if constexpr (sizeof(T) == 8)
+        v.val = reinterpret_cast<const T*>((which == 0 ? L.cA_v64 : which == 1 ? L.cP_v64 : L.cR_v64).data());
+    else
+        v.val = reinterpret_cast<const T*>((which == 0 ? L.cA_v32 : which == 1 ? L.cP_v32 : L.cR_v32).data());
+    return v;
+}
+
+template <typename T>
 void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     Level& L = levels_[l];
     auto buf = [&](DevBuf<double>& d64, DevBuf<float>& d32) -> T* {
@@ -437,14 +553,28 @@ void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     T* bc = buf(C.b64, C.b32);
     T* xc = buf(C.x64, C.x32);
     const T om = T(L.omega);
-    DevSell<T> A = view<T>(L, 0), P = view<T>(L, 1), R = view<T>(L, 2);
-    k_jacobi0<T><<<blocks(L.n), TPB, 0, s>>>(L.n, dinv, om, b, t);
-    k_residual<T><<<blocks(L.n), TPB, 0, s>>>(A, b, t, r);
-    k_spmv<T><<<blocks(C.n), TPB, 0, s>>>(R, r, bc);
-    launches += 3;
+    // pre-smoothing from zero + residual
+    if (L.A.csr)
+        launch_csr<T>(3, cview<T>(L, 0), dinv, om, b, nullptr, t, r, s);
+    else
+        k_jacobi0_residual<T><<<blocks(L.n), TPB, 0, s>>>(view<T>(L, 0), dinv, om, b, t, r);
+    // restriction
+    if (L.R.csr)
+        launch_csr<T>(0, cview<T>(L, 2), nullptr, T(0), nullptr, r, bc, nullptr, s);
+    else
+        k_spmv<T><<<blocks(C.n), TPB, 0, s>>>(view<T>(L, 2), r, bc);
+    launches += 2;
     cycle<T>(l + 1, bc, xc, s);
-    k_prolong_add<T><<<blocks(L.n), TPB, 0, s>>>(P, xc, t);
-    k_smooth<T><<<blocks(L.n), TPB, 0, s>>>(A, dinv, om, b, t, z);
+    // prolongation
+    if (L.P.csr)
+        launch_csr<T>(1, cview<T>(L, 1), nullptr, T(0), nullptr, xc, t, nullptr, s);
+    else
+        k_prolong_add<T><<<blocks(L.n), TPB, 0, s>>>(view<T>(L, 1), xc, t);
+    // post-smoothing
+    if (L.A.csr)
+        launch_csr<T>(2, cview<T>(L, 0), dinv, om, b, t, z, nullptr, s);
+    else
+        k_smooth<T><<<blocks(L.n), TPB, 0, s>>>(view<T>(L, 0), dinv, om, b, t, z);
     launches += 2;
 }
 

@@ -30,6 +30,16 @@ struct DevSell {
     const T* val = nullptr;
 };
 
+// CSR for matrices with long rows (restriction, coarse Galerkin operators): one group of G lanes
+// per row, G = the power of two nearest the mean row length (4..32)
+template <typename T>
+struct DevCsr {
+    int n = 0, group = 32;
+    const int* ptr = nullptr;
+    const int* col = nullptr;
+    const T* val = nullptr;
+};
+
 class Amg {
 public:
     // build the hierarchy of S (host CSR, symmetric positive definite or semi-definite)
@@ -48,6 +58,11 @@ private:
         std::vector<long long> soff;
         std::vector<int> width, col;
         std::vector<double> val;
+        // CSR copy used instead of the slices when rows are long
+        bool csr = false;
+        int group = 32;
+        std::vector<int> cptr, ccol;
+        std::vector<double> cval;
     };
     struct Level {
         int n = 0, nc = 0;
@@ -57,6 +72,9 @@ private:
         // device
         DevBuf<long long> dA_soff, dP_soff, dR_soff;
         DevBuf<int> dA_w, dA_col, dP_w, dP_col, dR_w, dR_col;
+        DevBuf<int> cA_ptr, cA_col, cP_ptr, cP_col, cR_ptr, cR_col;
+        DevBuf<double> cA_v64, cP_v64, cR_v64;
+        DevBuf<float> cA_v32, cP_v32, cR_v32;
         DevBuf<double> dA_v64, dP_v64, dR_v64, dinv64, x64, b64, r64, t64;
         DevBuf<float> dA_v32, dP_v32, dR_v32, dinv32, x32, b32, r32, t32;
     };
@@ -64,6 +82,8 @@ private:
     void cycle(int l, const T* b, T* z, cudaStream_t s);
     template <typename T>
     DevSell<T> view(const Level& L, int which) const;
+    template <typename T>
+    DevCsr<T> cview(const Level& L, int which) const;
 
     std::vector<Level> levels_;
     int ncoarse_ = 0;

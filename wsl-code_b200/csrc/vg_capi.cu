@@ -144,9 +144,9 @@ void vg_default_solve_opts(vg_solve_opts* o) {
     o->mode = VG_SOLVE_FP64;
     o->tol = 1e-10;
     o->maxit = 200000;
-    o->inner_tol = 1e-5;
+    o->inner_tol = 1e-6;
     o->max_outer = 12;
-    o->check_every = 32;
+    o->check_every = 0;
     o->nonzero_guess = 0;
 }
 

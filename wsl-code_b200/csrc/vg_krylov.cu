@@ -199,6 +199,12 @@ __global__ void __launch_bounds__(VEC_THREADS) k_step(MinresVecs<T> v, long long
     }
 }
 
+// end of one body of the graph's while loop: continue while not converged and below the cap
+__global__ void k_loop_check(cudaGraphConditionalHandle h, const int* flags, int* loop) {
+    int c = ++loop[0];
+    cudaGraphSetConditional(h, (flags[0] == 0 && c < loop[1]) ? 1u : 0u);
+}
+
 __global__ void __launch_bounds__(VEC_THREADS) k_residual64(const double* b, const double* y, double* r, long long n,
                                                             double* red, double* partials, unsigned* counter) {
     double acc[2] = {0, 0};
@@ -277,6 +283,11 @@ template void minres_finish<float>(const float*, const float*, long long, long l
                                    unsigned*, int, double, cudaStream_t);
 template void minres_step<double>(MinresVecs<double>, long long, Scalars*, int*, cudaStream_t);
 template void minres_step<float>(MinresVecs<float>, long long, Scalars*, int*, cudaStream_t);
+
+void loop_check(cudaGraphConditionalHandle h, const int* flags, int* loop, cudaStream_t s) {
+    k_loop_check<<<1, 1, 0, s>>>(h, flags, loop);
+    VG_CUDA(cudaGetLastError());
+}
 
 void residual64(const double* b, const double* y, double* r, long long n, double* red, double* partials,
                 unsigned* counter, cudaStream_t s) {

@@ -41,6 +41,8 @@ void minres_finish(const T* z, const T* v, long long plo, long long phi, Scalars
 template <typename T>
 void minres_step(MinresVecs<T> v, long long n, Scalars* sc, int* flags, cudaStream_t s);
 
+// graph while-loop condition: loop[0] = bodies run (incremented here), loop[1] = cap on bodies
+void loop_check(cudaGraphConditionalHandle h, const int* flags, int* loop, cudaStream_t s);
 // r = b - y (FP64), red[0] = ||r||^2, red[1] = ||b||^2 (deterministic)
 void residual64(const double* b, const double* y, double* r, long long n, double* red, double* partials,
                 unsigned* counter, cudaStream_t s);

@@ -259,11 +259,26 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
     d_counter_.zero();
     VG_CUDA(cudaEventCreate(&ev0_));
     VG_CUDA(cudaEventCreate(&ev1_));
+    VG_CUDA(cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming));
+    VG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    d_loop_.resize(2);
 }
 
 Solver::~Solver() {
+    destroy_graphs();
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
+    if (ev_in_) cudaEventDestroy(ev_in_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Solver::destroy_graphs() {
+    for (int p = 0; p < 2; ++p) {
+        if (gexec_[p]) cudaGraphExecDestroy(gexec_[p]);
+        if (graph_[p]) cudaGraphDestroy(graph_[p]);
+        gexec_[p] = nullptr;
+        graph_[p] = nullptr;
+    }
 }
 
 void Solver::pack_layout() {
@@ -449,6 +464,9 @@ void Solver::build() {
     }
     d_dinv64_.resize(N);
     d_dinv32_.resize(N);
+    destroy_graphs();
+    for (auto& b : sv64_) b.resize(N);
+    for (auto& b : sv32_) b.resize(N);
     make_diagonal(nullptr);
     // BC_FLUX: lifted right-hand side of MixedGpu::make_rhs (equation_gpu.cu:611-625):
     // free rows b - A g (unconstrained apply of the boundary values), boundary rows g
@@ -591,123 +609,129 @@ void Solver::rhs(double* b, cudaStream_t s) {
     VG_CUDA(cudaMemcpyAsync(b, d_rhs_.data(), sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
 }
 
-// MINRES on the symmetric constrained system K_sym x = r (x starts at zero)
-void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, int check_every, int& iters,
-                    cudaStream_t s) {
+template <>
+MinresVecs<float> Solver::vecs<float>(float* x) {
+    return MinresVecs<float>{w32_[0].data(), w32_[1].data(), w32_[2].data(), w32_[3].data(), w32_[4].data(),
+                             w32_[5].data(), w32_[6].data(), x, d_dinv32_.data()};
+}
+
+template <>
+MinresVecs<double> Solver::vecs<double>(double* x) {
+    return MinresVecs<double>{w64_[0].data(), w64_[1].data(), w64_[2].data(), w64_[3].data(), w64_[4].data(),
+                              w64_[5].data(), w64_[6].data(), x, d_dinv64_.data()};
+}
+
+template <typename T>
+ApplyArgs<T> Solver::apply_args(const T* x, T* y, bool constrained, T psign, double* quad, const int* flags) {
+    ApplyArgs<T> a{};
+    a.x = x;
+    a.y = y;
+    if constexpr (sizeof(T) == 8) {
+        a.A = d_A64_.data();
+        a.W = d_W64_.data();
+        a.L = d_L_.data();
+    } else {
+        a.A = d_A32_.data();
+        a.W = d_W32_.data();
+        a.L = d_L32_.data();
+    }
+    a.map = d_map_.data();
+    a.slot_cell = d_slot_cell_.data();
+    a.pieces = d_pieces_.data();
+    a.npieces = int(pieces_.size());
+    a.k = k;
+    a.mask = d_mask_.data();
+    a.flags = flags;
+    a.nf = nf;
+    a.N = N;
+    a.psign = psign;
+    a.constrained = (constrained && bc == VG_BC_FLUX) ? 1 : 0;
+    a.mult = bc == VG_BC_FLUX ? 1 : 0;
+    a.partials = d_partials_.data();
+    a.counter = d_counter_.data();
+    a.red = quad;
+    return a;
+}
+
+// one MINRES iteration: apply (with delta), update + preconditioner + gamma, step
+template <typename T>
+void Solver::iteration(MinresVecs<T>& v, cudaStream_t s) {
     Scalars* sc = reinterpret_cast<Scalars*>(d_scal_.data());
     int* flags = d_flags_.data();
-    const bool cons = bc == VG_BC_FLUX;
+    const long long plo = use_amg ? nf : 0, phi = use_amg ? nf + np : 0;
+    launch_apply(apply_args<T>(v.z_cur, v.y, true, T(-1), &sc->delta, flags), s);
+    minres_update<T>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s, plo, phi);
+    if (use_amg) {
+        amg_.vcycle(v.v_old + nf, v.z_new + nf, s);
+        minres_finish<T>(v.z_new, v.v_old, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(), 0, 0.0, s);
+    }
+    minres_step<T>(v, N, sc, flags, s);
+    std::swap(v.v_cur, v.v_old);
+    std::swap(v.z_cur, v.z_new);
+    std::swap(v.w_cur, v.w_old);
+}
+
+// the MINRES loop as a CUDA graph: a conditional while node whose body is two iterations (the
+// vector roles repeat with period two) followed by the condition kernel; the body count is capped
+// on the device, so the loop ends even if the convergence flag is never raised
+template <typename T>
+void Solver::build_graph(int p, T* x) {
+    VG_CUDA(cudaGraphCreate(&graph_[p], 0));
+    cudaGraphConditionalHandle h;
+    VG_CUDA(cudaGraphConditionalHandleCreate(&h, graph_[p], 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    VG_CUDA(cudaGraphAddNode(&node, graph_[p], nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    VG_CUDA(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    MinresVecs<T> v = vecs<T>(x);
+    const long long saved = amg_.launches;
+    try {
+        iteration<T>(v, stream_);
+        iteration<T>(v, stream_);
+        loop_check(h, d_flags_.data(), d_loop_.data(), stream_);
+    } catch (...) {
+        cudaGraph_t dummy;
+        cudaStreamEndCapture(stream_, &dummy);
+        throw;
+    }
+    amg_.launches = saved;
+    VG_CUDA(cudaStreamEndCapture(stream_, &body));
+    VG_CUDA(cudaGraphInstantiate(&gexec_[p], graph_[p], 0));
+}
+
+// MINRES on the symmetric constrained system K_sym x = r (x starts at zero)
+template <typename T>
+void Solver::minres_t(const T* r, T* x, double tol, int maxit, int check_every, int& iters, cudaStream_t s) {
+    Scalars* sc = reinterpret_cast<Scalars*>(d_scal_.data());
+    int* flags = d_flags_.data();
+    const int p = sizeof(T) == 4 ? 1 : 0;
+    const long long plo = use_amg ? nf : 0, phi = use_amg ? nf + np : 0;
+    const bool graph = check_every <= 0;
+    if (graph && !gexec_[p]) build_graph<T>(p, x);
+    MinresVecs<T> v = vecs<T>(x);
+    VG_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * N, s));
+    minres_init<T>(r, v, N, sc, flags, tol, d_partials_.data(), d_counter_.data(), s, plo, phi);
+    if (use_amg) {
+        amg_.vcycle(v.v_cur + nf, v.z_cur + nf, s);
+        minres_finish<T>(v.z_cur, v.v_cur, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(), 1, tol, s);
+    }
     int h_flags[NFLAGS] = {0, 0, 0, 0};
-    if (fp32) {
-        MinresVecs<float> v{w32_[0].data(), w32_[1].data(), w32_[2].data(), w32_[3].data(),
-                            w32_[4].data(), w32_[5].data(), w32_[6].data(), static_cast<float*>(x),
-                            d_dinv32_.data()};
-        VG_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * N, s));
-        const long long plo = use_amg ? nf : 0, phi = use_amg ? nf + np : 0;
-        minres_init<float>(static_cast<const float*>(r), v, N, sc, flags, tol, d_partials_.data(), d_counter_.data(), s,
-                           plo, phi);
-        if (use_amg) {
-            amg_.vcycle(v.v_cur + nf, v.z_cur + nf, s);
-            minres_finish<float>(v.z_cur, v.v_cur, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(), 1, tol, s);
-        }
-        int done = 0;
-        while (done < maxit) {
-            int batch = std::min(check_every, maxit - done);
-            for (int it = 0; it < batch; ++it) {
-                ApplyArgs<float> a{};
-                a.x = v.z_cur;
-                a.y = v.y;
-                a.A = d_A32_.data();
-                a.W = d_W32_.data();
-                a.map = d_map_.data();
-                a.slot_cell = d_slot_cell_.data();
-                a.pieces = d_pieces_.data();
-                a.npieces = int(pieces_.size());
-                a.k = k;
-                a.L = d_L32_.data();
-                a.mask = d_mask_.data();
-                a.flags = flags;
-                a.nf = nf;
-                a.N = N;
-                a.psign = -1.0f;
-                a.constrained = cons;
-                a.mult = cons;
-                a.partials = d_partials_.data();
-                a.counter = d_counter_.data();
-                a.red = &sc->delta;
-                launch_apply(a, s);
-                n_launch += 3;
-                ++n_apply;
-                minres_update<float>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s, plo, phi);
-                if (use_amg) {
-                    amg_.vcycle(v.v_old + nf, v.z_new + nf, s);
-                    minres_finish<float>(v.z_new, v.v_old, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(),
-                                         0, tol, s);
-                    n_launch += 1;
-                }
-                minres_step<float>(v, N, sc, flags, s);
-                std::swap(v.v_cur, v.v_old);
-                std::swap(v.z_cur, v.z_new);
-                std::swap(v.w_cur, v.w_old);
-            }
-            done += batch;
-            VG_CUDA(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, s));
-            VG_CUDA(cudaStreamSynchronize(s));
-            if (h_flags[0]) break;
-        }
+    if (graph) {
+        int loop[2] = {0, (maxit + 1) / 2};
+        VG_CUDA(cudaMemcpyAsync(d_loop_.data(), loop, sizeof(loop), cudaMemcpyHostToDevice, s));
+        VG_CUDA(cudaGraphLaunch(gexec_[p], s));
+        VG_CUDA(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, s));
+        VG_CUDA(cudaStreamSynchronize(s));
     } else {
-        MinresVecs<double> v{w64_[0].data(), w64_[1].data(), w64_[2].data(), w64_[3].data(),
-                             w64_[4].data(), w64_[5].data(), w64_[6].data(), static_cast<double*>(x),
-                             d_dinv64_.data()};
-        VG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
-        const long long plo = use_amg ? nf : 0, phi = use_amg ? nf + np : 0;
-        minres_init<double>(static_cast<const double*>(r), v, N, sc, flags, tol, d_partials_.data(), d_counter_.data(),
-                            s, plo, phi);
-        if (use_amg) {
-            amg_.vcycle(v.v_cur + nf, v.z_cur + nf, s);
-            minres_finish<double>(v.z_cur, v.v_cur, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(), 1, tol,
-                                  s);
-        }
-        int done = 0;
-        while (done < maxit) {
+        // host-driven batches of check_every iterations (every kernel is a plain launch)
+        for (int done = 0; done < maxit;) {
             int batch = std::min(check_every, maxit - done);
-            for (int it = 0; it < batch; ++it) {
-                ApplyArgs<double> a{};
-                a.x = v.z_cur;
-                a.y = v.y;
-                a.A = d_A64_.data();
-                a.W = d_W64_.data();
-                a.map = d_map_.data();
-                a.slot_cell = d_slot_cell_.data();
-                a.pieces = d_pieces_.data();
-                a.npieces = int(pieces_.size());
-                a.k = k;
-                a.L = d_L_.data();
-                a.mask = d_mask_.data();
-                a.flags = flags;
-                a.nf = nf;
-                a.N = N;
-                a.psign = -1.0;
-                a.constrained = cons;
-                a.mult = cons;
-                a.partials = d_partials_.data();
-                a.counter = d_counter_.data();
-                a.red = &sc->delta;
-                launch_apply(a, s);
-                n_launch += 3;
-                ++n_apply;
-                minres_update<double>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s, plo, phi);
-                if (use_amg) {
-                    amg_.vcycle(v.v_old + nf, v.z_new + nf, s);
-                    minres_finish<double>(v.z_new, v.v_old, plo, phi, sc, flags, d_partials_.data(),
-                                          d_counter_.data(), 0, tol, s);
-                    n_launch += 1;
-                }
-                minres_step<double>(v, N, sc, flags, s);
-                std::swap(v.v_cur, v.v_old);
-                std::swap(v.z_cur, v.z_new);
-                std::swap(v.w_cur, v.w_old);
-            }
+            for (int it = 0; it < batch; ++it) iteration<T>(v, s);
             done += batch;
             VG_CUDA(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, s));
             VG_CUDA(cudaStreamSynchronize(s));
@@ -715,20 +739,36 @@ void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, in
         }
     }
     iters = h_flags[2];
+    // kernels per iteration: apply, update, step (+ V-cycle and finish with multigrid)
+    const long long per = 3 + (use_amg ? 1 + 4LL * (amg_levels - 1) + 1 : 0);
+    n_launch += 2 + (use_amg ? 4LL * (amg_levels - 1) + 2 : 0) + per * iters + (iters + 2) / 2;
+    n_apply += iters;
     n_iter += iters;
-    n_launch += 1 + amg_.launches;  // init + multigrid cycles
-    amg_.launches = 0;
+}
+
+void Solver::minres(bool fp32, const void* r, void* x, double tol, int maxit, int check_every, int& iters,
+                    cudaStream_t s) {
+    if (fp32)
+        minres_t<float>(static_cast<const float*>(r), static_cast<float*>(x), tol, maxit, check_every, iters, s);
+    else
+        minres_t<double>(static_cast<const double*>(r), static_cast<double*>(x), tol, maxit, check_every, iters, s);
 }
 
 void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_info& info, cudaStream_t s) {
     if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_solve");
     if (!b || !x) throw Error(VG_EINVAL, "null vector");
-    if (!(o.tol > 0) || o.maxit < 1 || o.check_every < 1) throw Error(VG_EINVAL, "invalid solve options");
+    if (!(o.tol > 0) || o.maxit < 1 || o.check_every < 0 || (o.mode == VG_SOLVE_MIXED && !(o.inner_tol > 0 && o.inner_tol < 1)))
+        throw Error(VG_EINVAL, "invalid solve options");
     info = vg_solve_info{};
+    (void)s;
+    s = stream_;
+    // order after the caller's work on the legacy default stream
+    VG_CUDA(cudaEventRecord(ev_in_, nullptr));
+    VG_CUDA(cudaStreamWaitEvent(s, ev_in_, 0));
     VG_CUDA(cudaEventRecord(ev0_, s));
     const bool cons = bc == VG_BC_FLUX;
     // symmetric form: pressure / multiplier rows negated
-    DevBuf<double> bs(N), r(N), y(N), d(N);
+    DevBuf<double>&bs = sv64_[0], &r = sv64_[1], &y = sv64_[2], &d = sv64_[3];
     flip_pressure(b, bs.data(), nf, N, s);
     n_launch += 1;
     ++n_solve;
@@ -760,7 +800,7 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
             rel = true_residual();
         }
     } else {
-        DevBuf<float> r32(N), d32(N);
+        DevBuf<float>&r32 = sv32_[0], &d32 = sv32_[1];
         for (outer = 0; outer < o.max_outer && rel > o.tol && total < o.maxit; ++outer) {
             double rn = rel * nb;
             to_float(r.data(), r32.data(), 1.0 / rn, N, s);
@@ -795,10 +835,12 @@ void Solver::adjoint(const double* x, const double* dJdx, double* g, const vg_so
     // K_ref^T lambda = dJ/dx  <=>  K_sym mu = dJ/dx with mu = S lambda (S = diag(I, -I));
     // solve() takes a reference-sign right-hand side b and solves K_sym x = S b, so pass S dJ/dx
     DevBuf<double> rhs(N), mu(N);
-    flip_pressure(dJdx, rhs.data(), nf, N, s);
+    flip_pressure(dJdx, rhs.data(), nf, N, nullptr);
+    VG_CUDA(cudaDeviceSynchronize());
     vg_solve_opts oo = o;
     oo.nonzero_guess = 0;
     solve(rhs.data(), mu.data(), oo, info, s);
+    s = stream_;
     // dJ/dtheta_E = -lambda^T (dK/dtheta_E) x = mu_u,E^T A_E(theta) x_u,E  (dA_E/dtheta_E = -A_E)
     contract_adjoint(d_A64_.data(), d_map_.data(), d_slot_cell_.data(), d_mask_.data(), d_pieces_.data(),
                      int(pieces_.size()), k, x, mu.data(), bc == VG_BC_FLUX, g, s);

@@ -13,6 +13,8 @@
 
 #include "vg_common.cuh"
 #include "vg_amg.hpp"
+#include "vg_apply.cuh"
+#include "vg_krylov.cuh"
 #include "vg_setup.cuh"
 
 namespace vg {
@@ -75,6 +77,17 @@ private:
     void axpy64(double* x, const double* d, double a, cudaStream_t s);
     void minres(bool fp32, const void* b, void* x, double tol, int maxit, int check_every, int& iters,
                 cudaStream_t s);
+    template <typename T>
+    void minres_t(const T* r, T* x, double tol, int maxit, int check_every, int& iters, cudaStream_t s);
+    template <typename T>
+    MinresVecs<T> vecs(T* x);
+    template <typename T>
+    ApplyArgs<T> apply_args(const T* x, T* y, bool constrained, T psign, double* quad, const int* flags);
+    template <typename T>
+    void iteration(MinresVecs<T>& v, cudaStream_t s);
+    template <typename T>
+    void build_graph(int p, T* x);
+    void destroy_graphs();
 
     int device_ = 0;
     std::vector<Piece> pieces_;
@@ -110,6 +123,14 @@ private:
     DevBuf<int> d_flags_;
     SetupArgs setup_args_{};
     Amg amg_;
+    // solve workspaces (fixed addresses: the MINRES loop is a CUDA graph)
+    DevBuf<double> sv64_[4];
+    DevBuf<float> sv32_[2];
+    DevBuf<int> d_loop_;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev_in_ = nullptr;
+    cudaGraph_t graph_[2] = {nullptr, nullptr};
+    cudaGraphExec_t gexec_[2] = {nullptr, nullptr};
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
 };
 

@@ -132,7 +132,7 @@ class DarcyGpu:
         return b
 
     @staticmethod
-    def opts(mode="fp64", tol=1e-10, maxit=200000, inner_tol=1e-5, max_outer=12, check_every=32, guess=False):
+    def opts(mode="fp64", tol=1e-10, maxit=200000, inner_tol=1e-6, max_outer=12, check_every=0, guess=False):
         o = L.VgSolveOpts()
         L.lib().vg_default_solve_opts(ctypes.byref(o))
         o.mode = L.SOLVE_MIXED if mode == "mixed" else L.SOLVE_FP64
