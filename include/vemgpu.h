@@ -180,6 +180,19 @@ int vg_adjoint_grad(vg_handle* h, const double* x, const double* dJdx, double* d
  * flux L2 errors, physical scalar, flux and divergence L2 errors, physical mean-pressure mass. */
 int vg_errors(vg_handle* h, const double* x, double out[6]);
 
+/* vg_errors without any device allocation: the per-cell figures and their sums live in a
+ * static device array sized for VG_ERRORS_NOALLOC_MAX_CELLS cells (12.6 MB); larger meshes get
+ * VG_EINVAL. For callers that must not allocate device memory between solves: a process whose
+ * HBM is already reserved by its own caching allocator (cudaMalloc may fail there), or one that
+ * monitors the error inside a loop while other streams run (cudaMalloc and cudaFree can
+ * synchronize the device). Same results as vg_errors. The first call on a device looks up the
+ * array's address and must come before any stream capture on that device. The array is shared
+ * by every handle of a device, so calls that overlap on the GPU (several host threads) race.
+ * Runs on the legacy default stream and returns after the figures are on the host.
+ * No counterpart in the reference. */
+#define VG_ERRORS_NOALLOC_MAX_CELLS 262144
+int vg_errors_noalloc(vg_handle* h, const double* x, double out[6]);
+
 /* Copy one cell's local operator data to the host (verification): which = 0 A_E (n x n, K
  * included), 1 W_E (q x n), 2 P (p x n), 3 alpha (1), 4 global flux dof map with sign (n, as
  * doubles, sign * (index + 1)), 5 rhs (q), 6 Dirichlet load (n). Returns the count in *count. */

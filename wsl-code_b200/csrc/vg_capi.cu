@@ -202,6 +202,13 @@ int vg_errors(vg_handle* h, const double* x, double out[6]) {
     });
 }
 
+int vg_errors_noalloc(vg_handle* h, const double* x, double out[6]) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!x || !out) throw vg::Error(VG_EINVAL, "null vector");
+        s.errors_static(x, out);
+    });
+}
+
 int vg_local(vg_handle* h, int cell, int which, double* out, int* count) {
     return guarded(h, [&](vg::Solver& s) {
         int c = s.local(cell, which, out);

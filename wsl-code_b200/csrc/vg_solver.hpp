@@ -53,6 +53,8 @@ public:
     void adjoint(const double* x, const double* dJdx, double* g, const vg_solve_opts& o, vg_solve_info& info,
                  cudaStream_t s);
     void errors(const double* x, double out[6], cudaStream_t s);
+    // same figures with the per-cell scratch in a static device array (no device allocation)
+    void errors_static(const double* x, double out[6]);
     int local(int cell, int which, double* out);
 
     // sizes

@@ -74,6 +74,7 @@ def lib():
         L.vg_solve_host.argtypes = [P, P, P, ctypes.POINTER(VgSolveOpts), ctypes.POINTER(VgSolveInfo)]
         L.vg_adjoint_grad.argtypes = [P, P, P, P, ctypes.POINTER(VgSolveOpts), ctypes.POINTER(VgSolveInfo)]
         L.vg_errors.argtypes = [P, P, P]
+        L.vg_errors_noalloc.argtypes = [P, P, P]
         L.vg_local.argtypes = [P, I, I, P, ctypes.POINTER(I)]
         L.vg_stats.argtypes = [P, P]
         _lib = L
