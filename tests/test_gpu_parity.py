@@ -117,6 +117,43 @@ def test_apply_arcs_pressure_bc(disk200, k):
     _close(g.rhs().cpu().numpy(), b, 1e-12)
 
 
+def _polar_mesh(rings=3, sectors=16, r0=0.2):
+    """A 16-gon centre cell inside rings of quadrilaterals: its operator record exceeds a
+    shared-memory stage, so the apply reads it from the strided arrays."""
+    r = np.linspace(r0, 1.0, rings + 1)
+    t = 2 * np.pi * np.arange(sectors) / sectors
+    xy = np.concatenate([np.stack([ri * np.cos(t), ri * np.sin(t)], 1) for ri in r])
+    cells = [list(range(sectors))]
+    for i in range(rings):
+        for j in range(sectors):
+            a, b = i * sectors + j, i * sectors + (j + 1) % sectors
+            cells.append([a, b, b + sectors, a + sectors])
+    ptr = np.cumsum([0] + [len(c) for c in cells])
+    return dict(xy=xy, cell_ptr=ptr, cell_nodes=np.concatenate(cells))
+
+
+@pytest.mark.parametrize("k", [0, 1])
+@pytest.mark.parametrize("constrained", [False, True])
+def test_apply_large_polygon_record(k, constrained):
+    o, g = pair(_polar_mesh(), k, 9, O.GEOM_IDENTITY, 0.0, O.PROB_SINCOS, O.BC_FLUX)
+    x, y, ref = _apply_case(o, g, constrained)
+    _close(y, ref, 1e-12)
+    y32 = g.apply(torch.from_numpy(x).float().cuda(), constrained=constrained).double().cpu().numpy()
+    _close(y32, ref, 2e-6)
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_apply_many_ctas_matches_oracle(k):
+    """Enough pieces for every CTA of the streamed apply to own several stages."""
+    m = meshgen.voronoi_mesh(20000 if k == 0 else 8000, "annulus", seed=21)
+    th = np.random.default_rng(22).normal(0, 1.5, len(m["cell_ptr"]) - 1)
+    o, g = pair(m, k, 9, O.GEOM_ARCS, 0.0, O.PROB_ANNULUS, O.BC_PRESSURE, theta=th)
+    x, y, ref = _apply_case(o, g, True)
+    _close(y, ref, 1e-12)
+    y32 = g.apply(torch.from_numpy(x).float().cuda()).double().cpu().numpy()
+    _close(y32, ref, 2e-6)
+
+
 def test_apply_is_deterministic(disk200):
     _, g = pair(disk200, 0, 9, O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
     x = torch.randn(g.N, dtype=torch.float64, device="cuda")

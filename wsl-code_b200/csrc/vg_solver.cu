@@ -190,6 +190,7 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
     if (ndev == 0) throw Error(VG_ECUDA, "no CUDA device");
     if (device >= 0) VG_CUDA(cudaSetDevice(device));
     VG_CUDA(cudaGetDevice(&device_));
+    VG_CUDA(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
     q = dimP(k);
     p = p_of(k);
     ngrad = ngrad_of(k);
@@ -247,6 +248,7 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
     d_cell_slot_.upload(cell_slot_);
     d_pieces_.upload(pieces_);
     d_map_.upload(map_host_);
+    plan_streams();
     {
         std::vector<int> occ(m.eocc);
         DevBuf<int> tmp;
@@ -371,6 +373,7 @@ void Solver::set_theta(const double* theta, bool on_device) {
     if (built) {
         rescale_ops(d_theta_.data(), d_slot_cell_.data(), d_pieces_.data(), int(pieces_.size()), d_A0_.data(),
                     d_A64_.data(), d_A32_.data(), nullptr);
+        pack_streams(nullptr);
         make_diagonal(nullptr);
         VG_CUDA(cudaDeviceSynchronize());
     }
@@ -454,6 +457,7 @@ void Solver::build() {
     for (const auto& c : classes_) launch_setup(a, c, nqp, nullptr);
     VG_CUDA(cudaDeviceSynchronize());
     check_status("setup");
+    pack_streams(nullptr);
     // workspaces
     d_partials_.resize(2 * size_t(std::max(apply_blocks(int(pieces_.size())), VEC_BLOCKS)) + 16);
     d_red_.resize(8);
@@ -553,57 +557,54 @@ void Solver::build_amg() {
 }
 
 void Solver::apply64(const double* x, double* y, bool constrained, double psign, cudaStream_t s, double* quad) {
-    ApplyArgs<double> a{};
-    a.x = x;
-    a.y = y;
-    a.A = d_A64_.data();
-    a.W = d_W64_.data();
-    a.map = d_map_.data();
-    a.slot_cell = d_slot_cell_.data();
-    a.pieces = d_pieces_.data();
-    a.npieces = int(pieces_.size());
-    a.k = k;
-    a.L = d_L_.data();
-    a.mask = d_mask_.data();
-    a.flags = nullptr;
-    a.nf = nf;
-    a.N = N;
-    a.psign = psign;
-    a.constrained = (constrained && bc == VG_BC_FLUX) ? 1 : 0;
-    a.mult = bc == VG_BC_FLUX ? 1 : 0;
-    a.partials = d_partials_.data();
-    a.counter = d_counter_.data();
-    a.red = quad;
-    launch_apply(a, s);
+    launch_apply(apply_args<double>(x, y, constrained, psign, quad, nullptr), s);
     n_launch += 1;
     ++n_apply;
 }
 
 void Solver::apply32(const float* x, float* y, bool constrained, float psign, cudaStream_t s, double* quad) {
-    ApplyArgs<float> a{};
-    a.x = x;
-    a.y = y;
-    a.A = d_A32_.data();
-    a.W = d_W32_.data();
-    a.map = d_map_.data();
-    a.slot_cell = d_slot_cell_.data();
-    a.pieces = d_pieces_.data();
-    a.npieces = int(pieces_.size());
-    a.k = k;
-    a.L = d_L32_.data();
-    a.mask = d_mask_.data();
-    a.flags = nullptr;
-    a.nf = nf;
-    a.N = N;
-    a.psign = psign;
-    a.constrained = (constrained && bc == VG_BC_FLUX) ? 1 : 0;
-    a.mult = bc == VG_BC_FLUX ? 1 : 0;
-    a.partials = d_partials_.data();
-    a.counter = d_counter_.data();
-    a.red = quad;
-    launch_apply(a, s);
+    launch_apply(apply_args<float>(x, y, constrained, psign, quad, nullptr), s);
     n_launch += 1;
     ++n_apply;
+}
+
+void Solver::plan_streams() {
+    if (k > 1) return;
+    plan64_ = plan_stream(pieces_, k, 8, sm_count_);
+    plan32_ = plan_stream(pieces_, k, 4, sm_count_);
+    d_rec64_.resize(size_t(plan64_.bytes));
+    d_rec32_.resize(size_t(plan32_.bytes));
+    d_roff64_.upload(plan64_.rec_off);
+    d_roff32_.upload(plan32_.rec_off);
+    d_bat64_.upload(plan64_.batches);
+    d_bat32_.upload(plan32_.batches);
+    d_cta64_.upload(plan64_.cta_batch);
+    d_cta32_.upload(plan32_.cta_batch);
+    d_err_.resize(1);
+    d_err_.zero();
+    prepare_stream_kernels();
+}
+
+void Solver::pack_streams(cudaStream_t s) {
+    if (k > 1) return;
+    const int np_ = int(pieces_.size());
+    pack_stream<double>(d_pieces_.data(), np_, d_roff64_.data(), d_A64_.data(), d_W64_.data(), d_map_.data(),
+                        d_slot_cell_.data(), k, d_rec64_.data(), s);
+    pack_stream<float>(d_pieces_.data(), np_, d_roff32_.data(), d_A32_.data(), d_W32_.data(), d_map_.data(),
+                       d_slot_cell_.data(), k, d_rec32_.data(), s);
+    VG_CUDA(cudaStreamSynchronize(s));
+}
+
+// the bulk-copy apply sets the error word when a pipeline wait gave up (never in a correct run)
+void Solver::check_pipeline() {
+    if (k > 1) return;
+    int e = 0;
+    VG_CUDA(cudaMemcpy(&e, d_err_.data(), sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        d_err_.zero();
+        VG_CUDA(cudaDeviceSynchronize());
+        throw Error(VG_ECUDA, "apply pipeline wait timed out");
+    }
 }
 
 void Solver::rhs(double* b, cudaStream_t s) {
@@ -651,6 +652,16 @@ ApplyArgs<T> Solver::apply_args(const T* x, T* y, bool constrained, T psign, dou
     a.partials = d_partials_.data();
     a.counter = d_counter_.data();
     a.red = quad;
+    if (k <= 1 && d_err_.data()) {
+        const StreamPlan& pl = sizeof(T) == 8 ? plan64_ : plan32_;
+        a.rec = sizeof(T) == 8 ? d_rec64_.data() : d_rec32_.data();
+        a.batches = sizeof(T) == 8 ? d_bat64_.data() : d_bat32_.data();
+        a.cta_batch = sizeof(T) == 8 ? d_cta64_.data() : d_cta32_.data();
+        a.ncta = pl.ncta;
+        a.stages = pl.stages;
+        a.stage_bytes = pl.stage_bytes;
+        a.err = d_err_.data();
+    }
     return a;
 }
 
@@ -815,6 +826,7 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
     }
     VG_CUDA(cudaEventRecord(ev1_, s));
     VG_CUDA(cudaEventSynchronize(ev1_));
+    check_pipeline();
     float ms = 0;
     VG_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
     info.iterations = total;

@@ -73,6 +73,9 @@ public:
 
 private:
     void pack_layout();
+    void plan_streams();
+    void pack_streams(cudaStream_t s);
+    void check_pipeline();
     void make_diagonal(cudaStream_t s);
     void build_amg();
     void check_status(const char* where);
@@ -134,6 +137,14 @@ private:
     cudaGraph_t graph_[2] = {nullptr, nullptr};
     cudaGraphExec_t gexec_[2] = {nullptr, nullptr};
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    // record streams of the bulk-copy apply (k <= 1), one per precision
+    int sm_count_ = 0;
+    StreamPlan plan64_, plan32_;
+    DevBuf<unsigned char> d_rec64_, d_rec32_;
+    DevBuf<long long> d_roff64_, d_roff32_;
+    DevBuf<ApplyBatch> d_bat64_, d_bat32_;
+    DevBuf<int> d_cta64_, d_cta32_;
+    DevBuf<int> d_err_;
 };
 
 }  // namespace vg
