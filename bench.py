@@ -34,7 +34,7 @@ INNER_TOL = 1e-6  # FP32 inner MINRES: relative reduction per refinement step
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=1_000_000)
@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--profile", action="store_true", help="short fixed run for profilers (applies + 2 solves)")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient workload")
+    ap.add_argument("--adjoint-cells", type=int, default=250000)
     ap.add_argument("--eager", action="store_true", help="with --profile: host-driven Krylov batches, no graph")
     return ap.parse_args()
 
@@ -173,6 +175,62 @@ def reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_leg(args, rank):
+    """Gradient workload: 250k-cell annulus, lognormal K, J = sum over 64 seeded interior points
+    of (p_h - d)^2. Reports the adjoint (vg_adjoint_grad: adjoint solve + per-cell contraction)
+    against the forward solve, both device-timed, and central differences (step 1e-6) of J along two
+    seeded unit directions against the adjoint's directional derivative."""
+    import numpy as np
+    import torch
+    import vemgpu
+    from vemgpu import fields, observe
+    from vemgpu.autograd import darcy_solve
+    cells = args.adjoint_cells
+    mesh, _ = annulus_problem(cells, args.seed)
+    th = fields.gaussian_field(fields.cell_centroids(mesh), sigma=2.0, corr=0.1, seed=args.seed + 11 + rank)
+    h = vemgpu.DarcyGpu(mesh, k=0, nq=9, ng=9, geometry="arcs", problem="annulus", bc="pressure", theta=th)
+    obs = observe.PointObservation(h, mesh, observe.seeded_points(64, args.seed + 12),
+                                   data=np.random.default_rng(args.seed + 13).uniform(0.2, 0.8, 64))
+    out = {"cells": h.nc, "observations": 64}
+    for mode in ("mixed", "fp64"):
+        opts = dict(mode=mode, tol=1e-10, inner_tol=INNER_TOL)
+        fw, ad = [], []
+        for i in range(4):
+            x, info = h.solve(**opts)
+            J = obs(x)
+            dJdx = torch.autograd.functional.vjp(obs, x)[1]
+            g, ainfo = h.adjoint_grad(x, dJdx, **opts)
+            if i:
+                fw.append(info["seconds"])
+                ad.append(ainfo["seconds"])
+        torch.cuda.synchronize()
+        out[mode] = {"forward_s": float(np.mean(fw)), "adjoint_s": float(np.mean(ad)),
+                     "grad_over_solve": float(np.mean(ad) / np.mean(fw)),
+                     "forward_iterations": info["iterations"], "adjoint_iterations": ainfo["iterations"]}
+    # central differences of J (FP64 solves to 1e-12) against the adjoint directional derivative
+    theta = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
+    J = obs(darcy_solve(h, theta, tol=1e-12))
+    J.backward()
+    rng = np.random.default_rng(args.seed + 14)
+    gn = float(torch.linalg.norm(theta.grad))
+    fd = []
+    with torch.no_grad():
+        # the gradient direction (derivative = |g|) and one seeded random unit direction
+        for name, v in (("gradient", theta.grad / gn),
+                        ("random", torch.tensor(rng.standard_normal(h.nc), device="cuda"))):
+            v = v / torch.linalg.norm(v)
+            jp = float(obs(darcy_solve(h, theta + 1e-6 * v, tol=1e-12)))
+            jm = float(obs(darcy_solve(h, theta - 1e-6 * v, tol=1e-12)))
+            dd, cd = float(theta.grad @ v), (jp - jm) / 2e-6
+            fd.append({"direction": name, "adjoint": dd, "central_difference": cd,
+                       "diff_over_grad_norm": abs(dd - cd) / gn})
+    out["fd_check"] = fd
+    out["grad_norm"] = gn
+    out["J"] = float(J.detach())
+    h.close()
+    return out
+
+
 def ours(args, rank, world, dist):
     import numpy as np
     import torch
@@ -292,11 +350,14 @@ def ours(args, rank, world, dist):
     ach32 = b32 / (apply32_ms * 1e-3) / 1e9
     ach64 = b64 / (apply64_ms * 1e-3) / 1e9
     # end to end through the host-buffer C ABI call (H2D of b and D2H of x inside)
-    bh = b.cpu().numpy()
+    bh_t = torch.empty(g.N, dtype=torch.float64, pin_memory=True)
+    bh_t.copy_(b)
+    xh_t = torch.empty(g.N, dtype=torch.float64, pin_memory=True)
+    bh, xh = bh_t.numpy(), xh_t.numpy()
     e2e = []
     for i in range(1 + args.steps):
         t = time.perf_counter()
-        xh, info_h = g.solve_host(bh, mode="mixed", tol=1e-10, inner_tol=INNER_TOL)
+        _, info_h = g.solve_host(bh, out=xh, mode="mixed", tol=1e-10, inner_tol=INNER_TOL)
         if i:
             e2e.append(time.perf_counter() - t)
     e2e_s = sum(e2e) / len(e2e)
@@ -304,6 +365,7 @@ def ours(args, rank, world, dist):
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_s = float(t.item())
+    adjoint = None if args.no_adjoint else adjoint_leg(args, rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
         threads = 1
@@ -337,6 +399,7 @@ def ours(args, rank, world, dist):
                      "peak_kind": peak_kind, "fp64_apply_frac": ach64 / peak,
                      "fp64_traffic": traffic_bytes("apply_bulk_kernel<double, 0>", g.nc)},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * g.N, "d2h_bytes_per_step": 8 * g.N},
+        "adjoint": adjoint,
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,

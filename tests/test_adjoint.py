@@ -1,0 +1,197 @@
+"""Adjoint gradient dJ/dtheta of point observations of the pressure (log permeability theta per
+cell), through the torch.autograd.Function over vg_solve / vg_adjoint_grad.
+
+Checks, with the tolerance of each written in the test:
+* against the CPU FP64 adjoint of the oracle (sparse LU on the assembled system, the per-cell
+  contraction lambda_E^T A_E u_E with the oracle's own dof map and signs): relative 1e-8;
+* against central finite differences (step 1e-6, 20 seeded unit directions) of J computed by the
+  GPU solver at tolerance 1e-12: relative 1e-6 of the largest directional derivative;
+* against central finite differences (step 1e-6) of J computed by the oracle's direct solver (no
+  Krylov error): 1e-6 of the gradient norm.
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import vemgpu  # noqa: E402
+from vemgpu import fields, meshgen, observe  # noqa: E402
+from vemgpu.autograd import darcy_solve  # noqa: E402
+
+GEO = {O.GEOM_IDENTITY: "identity", O.GEOM_SINE: "sine", O.GEOM_ARCS: "arcs"}
+
+
+@pytest.fixture(scope="module")
+def annulus2k():
+    m = meshgen.voronoi_mesh(2000, "annulus", seed=31)
+    th = fields.gaussian_field(fields.cell_centroids(m), sigma=1.0, corr=0.2, seed=32)
+    pts = observe.seeded_points(16, 33)
+    return m, th, pts
+
+
+def _oracle_J_and_grad(m, th, k, cells, data, problem=O.PROB_ANNULUS, bc=O.BC_PRESSURE, geom=O.GEOM_ARCS,
+                       eps=0.0):
+    o = O.Oracle(m, k=k, nq=9, ng=9, geom=geom, eps=eps, problem=problem, bc=bc, theta=th)
+    K, b = o.system()
+    if bc == O.BC_FLUX:
+        # essential flux rows: K_c = Q K Q + (I - Q), b_c = Q (b - K g) + g (MixedGpu::make_rhs lift)
+        import scipy.sparse as sp
+        msk, gv = o.boundary()
+        Q = sp.diags((~msk).astype(float))
+        K = (Q @ K @ Q + sp.diags(msk.astype(float))).tocsr()
+        b = np.where(msk, gv, b - o.system()[0] @ gv)
+    lu = spla.splu(K.tocsc())
+    x = lu.solve(b)
+    q = (k + 1) * (k + 2) // 2
+    idx = o.nf + cells * q
+    r = x[idx] - data
+    J = float(r @ r)
+    dJdx = np.zeros(o.N)
+    np.add.at(dJdx, idx, 2 * r)
+    lam = lu.solve(dJdx, trans="T")
+    g = np.zeros(o.nc)
+    mask = o.boundary()[0] if bc == O.BC_FLUX else np.zeros(o.N, bool)
+    for c in range(o.nc):
+        d = o.local(c, "dir")
+        n = len(d)
+        gd = o.local(c, "gdofs")[:n].astype(np.int64)
+        A = o.local(c, "A").reshape(n, n)
+        u = d * x[gd]
+        w = np.where(mask[gd], 0.0, d * lam[gd])
+        g[c] = w @ A @ u
+    return J, g, x
+
+
+def _gpu_J(h, obs, theta, tol):
+    x = darcy_solve(h, theta, tol=tol)
+    return obs(x)
+
+
+def test_gradient_matches_cpu_adjoint(annulus2k):
+    m, th, pts = annulus2k
+    h = vemgpu.DarcyGpu(m, k=0, geometry="arcs", problem="annulus", bc="pressure", theta=th)
+    obs = observe.PointObservation(h, m, pts, data=np.linspace(0.2, 0.8, len(pts)))
+    theta = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
+    J = _gpu_J(h, obs, theta, 1e-12)
+    J.backward()
+    Jc, gc, _ = _oracle_J_and_grad(m, th, 0, obs.cells, obs.data.cpu().numpy())
+    assert float(J.detach()) == pytest.approx(Jc, rel=1e-9)
+    g = theta.grad.cpu().numpy()
+    assert np.abs(g - gc).max() <= 1e-8 * np.abs(gc).max()
+    h.close()
+
+
+def test_gradient_matches_central_differences(annulus2k):
+    m, th, pts = annulus2k
+    h = vemgpu.DarcyGpu(m, k=0, geometry="arcs", problem="annulus", bc="pressure", theta=th)
+    obs = observe.PointObservation(h, m, pts, data=np.linspace(0.2, 0.8, len(pts)))
+    theta = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
+    J = _gpu_J(h, obs, theta, 1e-12)
+    J.backward()
+    g = theta.grad.clone()
+    rng = np.random.default_rng(34)
+    step = 1e-6
+    ad, fd = [], []
+    with torch.no_grad():
+        for _ in range(20):
+            v = rng.standard_normal(len(th))
+            v /= np.linalg.norm(v)
+            vt = torch.tensor(v, dtype=torch.float64, device="cuda")
+            jp = float(_gpu_J(h, obs, theta + step * vt, 1e-12))
+            jm = float(_gpu_J(h, obs, theta - step * vt, 1e-12))
+            fd.append((jp - jm) / (2 * step))
+            ad.append(float(g @ vt))
+    ad, fd = np.array(ad), np.array(fd)
+    assert np.abs(ad - fd).max() <= 1e-6 * np.abs(ad).max(), (ad, fd)
+    h.close()
+
+
+def test_gradient_matches_oracle_differences_k1():
+    m = meshgen.voronoi_mesh(400, "disk", seed=41)
+    th = fields.gaussian_field(fields.cell_centroids(m), sigma=1.0, corr=0.3, seed=42)
+    pts = observe.seeded_points(8, 43, r_in=0.0, r_out=0.9)
+    cells = observe.locate_cells(m, pts)
+    data = np.full(len(pts), 0.1)
+    h = vemgpu.DarcyGpu(m, k=1, geometry="arcs", problem="sinsin", bc="pressure", theta=th)
+    q = 3
+    idx = torch.as_tensor(h.nf + cells * q, dtype=torch.long, device="cuda")  # mean-moment unknown
+    theta = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
+    x = darcy_solve(h, theta, tol=1e-12)
+    J = ((x[idx] - torch.as_tensor(data, device="cuda")) ** 2).sum()
+    J.backward()
+    g = theta.grad.cpu().numpy()
+    J0, gc, _ = _oracle_J_and_grad(m, th, 1, cells, data, problem=O.PROB_SINSIN)
+    assert float(J.detach()) == pytest.approx(J0, rel=1e-9)
+    assert np.abs(g - gc).max() <= 1e-8 * np.abs(gc).max()
+    # oracle central differences (step 1e-6) along 3 unit directions (direct solves: no Krylov
+    # tolerance in J); with J ~ 10 the rounding of J alone gives ~1e-8 absolute noise in the quotient,
+    # so the bound is 1e-6 of the gradient norm (|g.v| <= |g| for a unit v)
+    rng = np.random.default_rng(44)
+    for _ in range(3):
+        v = rng.standard_normal(len(th))
+        v /= np.linalg.norm(v)
+        jp = _oracle_J_and_grad(m, th + 1e-6 * v, 1, cells, data, problem=O.PROB_SINSIN)[0]
+        jm = _oracle_J_and_grad(m, th - 1e-6 * v, 1, cells, data, problem=O.PROB_SINSIN)[0]
+        assert abs((jp - jm) / 2e-6 - g @ v) <= 1e-6 * np.linalg.norm(g)
+    h.close()
+
+
+def test_gradient_flux_bc_matches_cpu_adjoint(square_meshes):
+    m = square_meshes["square_4x4"]
+    nc = len(m["cell_ptr"]) - 1
+    th = np.random.default_rng(51).normal(0, 0.5, nc)
+    h = vemgpu.DarcyGpu(m, k=1, geometry="sine", eps=0.05, problem="sincos", bc="flux", theta=th)
+    cells = np.arange(0, nc, 5)
+    data = np.zeros(len(cells))
+    idx = torch.as_tensor(h.nf + cells * 3, dtype=torch.long, device="cuda")
+    theta = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
+    x = darcy_solve(h, theta, tol=1e-12)
+    J = (x[idx] ** 2).sum()
+    J.backward()
+    J0, gc, xo = _oracle_J_and_grad(m, th, 1, cells, data, problem=O.PROB_SINCOS, bc=O.BC_FLUX,
+                                    geom=O.GEOM_SINE, eps=0.05)
+    assert np.linalg.norm(x.detach().cpu().numpy() - xo) <= 1e-9 * np.linalg.norm(xo)
+    g = theta.grad.cpu().numpy()
+    assert np.abs(g - gc).max() <= 1e-8 * np.abs(gc).max()
+    h.close()
+
+
+def test_theta_update_after_build_matches_fresh_handle(square_meshes):
+    """vg_set_log_permeability after vg_build (operator rescale, preconditioner and the lifted
+    essential-BC right-hand side) gives the same solution as a handle built with that theta."""
+    m = square_meshes["square_4x4"]
+    nc = len(m["cell_ptr"]) - 1
+    th = np.random.default_rng(52).normal(0, 0.7, nc)
+    a = vemgpu.DarcyGpu(m, k=1, geometry="sine", eps=0.05, problem="sincos", bc="flux")
+    a.set_log_permeability(th)
+    b = vemgpu.DarcyGpu(m, k=1, geometry="sine", eps=0.05, problem="sincos", bc="flux", theta=th)
+    xa, _ = a.solve(tol=1e-12)
+    xb, _ = b.solve(tol=1e-12)
+    assert torch.allclose(a.rhs(), b.rhs(), rtol=1e-13, atol=1e-14)
+    assert torch.linalg.norm(xa - xb) <= 1e-10 * torch.linalg.norm(xb)
+    a.close()
+    b.close()
+
+
+def test_theta_update_rebuilds_multigrid(annulus2k):
+    """k = 0 with the pressure condition: a permeability update after a graph-captured solve
+    rebuilds the multigrid hierarchy (and the captured Krylov loop) before the next solve."""
+    m, th, _ = annulus2k
+    a = vemgpu.DarcyGpu(m, k=0, geometry="arcs", problem="annulus", bc="pressure")
+    a.solve(tol=1e-10)
+    for mode in ("fp64", "mixed"):
+        a.solve(tol=1e-10, mode=mode)
+    a.set_log_permeability(th)
+    b = vemgpu.DarcyGpu(m, k=0, geometry="arcs", problem="annulus", bc="pressure", theta=th)
+    for mode in ("fp64", "mixed"):
+        xa, ia = a.solve(tol=1e-10, mode=mode)
+        xb, ib = b.solve(tol=1e-10, mode=mode)
+        assert ia["residual"] <= 1e-10 and ib["residual"] <= 1e-10
+        assert ia["iterations"] == ib["iterations"]
+        assert torch.linalg.norm(xa - xb) <= 1e-9 * torch.linalg.norm(xb)
+    a.close()
+    b.close()

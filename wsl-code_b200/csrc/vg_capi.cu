@@ -172,12 +172,8 @@ int vg_solve_host(vg_handle* h, const double* b_host, double* x_host, const vg_s
         vg_solve_opts o;
         vg_default_solve_opts(&o);
         if (opts) o = *opts;
-        vg::DevBuf<double> b(s.N), x(s.N);
-        VG_CUDA(cudaMemcpy(b.data(), b_host, sizeof(double) * s.N, cudaMemcpyHostToDevice));
-        if (o.nonzero_guess) VG_CUDA(cudaMemcpy(x.data(), x_host, sizeof(double) * s.N, cudaMemcpyHostToDevice));
         vg_solve_info inf{};
-        s.solve(b.data(), x.data(), o, inf, nullptr);
-        VG_CUDA(cudaMemcpy(x_host, x.data(), sizeof(double) * s.N, cudaMemcpyDeviceToHost));
+        s.solve_host(b_host, x_host, o, inf);
         if (info) *info = inf;
     });
 }

@@ -375,6 +375,7 @@ void Solver::set_theta(const double* theta, bool on_device) {
                     d_A64_.data(), d_A32_.data(), nullptr);
         pack_streams(nullptr);
         make_diagonal(nullptr);
+        lift_flux_rhs();
         VG_CUDA(cudaDeviceSynchronize());
     }
 }
@@ -475,14 +476,22 @@ void Solver::build() {
     make_diagonal(nullptr);
     // BC_FLUX: lifted right-hand side of MixedGpu::make_rhs (equation_gpu.cu:611-625):
     // free rows b - A g (unconstrained apply of the boundary values), boundary rows g
-    if (bc == VG_BC_FLUX) {
-        double* y = w64_[0].data();
-        w64_[0].zero();
-        apply64(d_bval_.data(), y, false, 1.0, nullptr);
-        lift_rhs(d_mask_.data(), d_bval_.data(), y, d_rhs_.data(), N, nullptr);
-    }
+    d_rhs0_.resize(N);
+    VG_CUDA(cudaMemcpy(d_rhs0_.data(), d_rhs_.data(), sizeof(double) * N, cudaMemcpyDeviceToDevice));
+    lift_flux_rhs();
     VG_CUDA(cudaDeviceSynchronize());
     built = true;
+}
+
+// BC_FLUX: the lifted right-hand side depends on the operator (b - A g), so it is recomputed from
+// the unlifted one whenever the permeability changes
+void Solver::lift_flux_rhs() {
+    if (bc != VG_BC_FLUX) return;
+    VG_CUDA(cudaMemcpy(d_rhs_.data(), d_rhs0_.data(), sizeof(double) * N, cudaMemcpyDeviceToDevice));
+    double* y = w64_[0].data();
+    w64_[0].zero();
+    apply64(d_bval_.data(), y, false, 1.0, nullptr);
+    lift_rhs(d_mask_.data(), d_bval_.data(), y, d_rhs_.data(), N, nullptr);
 }
 
 void Solver::make_diagonal(cudaStream_t s) {
@@ -499,6 +508,9 @@ void Solver::make_diagonal(cudaStream_t s) {
                 bc == VG_BC_FLUX, N, s);
     to_float_plain(d_dinv64_.data(), d_dinv32_.data(), N, s);
     VG_CUDA(cudaStreamSynchronize(s));
+    // the captured Krylov loops hold the multigrid hierarchy's device addresses, which the rebuild
+    // below frees: drop them (they are captured again by the next solve)
+    destroy_graphs();
     use_amg = false;
     if (k == 0 && bc == VG_BC_PRESSURE) build_amg();
 }
@@ -838,6 +850,20 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
                                     " true_relative_residual=" + std::to_string(rel));
 }
 
+void Solver::solve_host(const double* b_host, double* x_host, const vg_solve_opts& o, vg_solve_info& info) {
+    if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_solve_host");
+    d_hb_.resize(N);
+    d_hx_.resize(N);
+    // copies on the solver stream: solve() orders its own work after the legacy stream, so the
+    // inputs are enqueued there first
+    VG_CUDA(cudaMemcpyAsync(d_hb_.data(), b_host, sizeof(double) * N, cudaMemcpyHostToDevice, nullptr));
+    if (o.nonzero_guess)
+        VG_CUDA(cudaMemcpyAsync(d_hx_.data(), x_host, sizeof(double) * N, cudaMemcpyHostToDevice, nullptr));
+    solve(d_hb_.data(), d_hx_.data(), o, info, nullptr);
+    VG_CUDA(cudaMemcpyAsync(x_host, d_hx_.data(), sizeof(double) * N, cudaMemcpyDeviceToHost, stream_));
+    VG_CUDA(cudaStreamSynchronize(stream_));
+}
+
 void Solver::axpy64(double* x, const double* d, double a, cudaStream_t s) {
     axpy64_kernel_launch(x, d, a, N, s);
 }
@@ -847,9 +873,10 @@ void Solver::adjoint(const double* x, const double* dJdx, double* g, const vg_so
     if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_adjoint_grad");
     // K_ref^T lambda = dJ/dx  <=>  K_sym mu = dJ/dx with mu = S lambda (S = diag(I, -I));
     // solve() takes a reference-sign right-hand side b and solves K_sym x = S b, so pass S dJ/dx
-    DevBuf<double> rhs(N), mu(N);
-    flip_pressure(dJdx, rhs.data(), nf, N, nullptr);
-    VG_CUDA(cudaDeviceSynchronize());
+    d_adj_rhs_.resize(N);
+    d_adj_mu_.resize(N);
+    DevBuf<double>&rhs = d_adj_rhs_, &mu = d_adj_mu_;
+    flip_pressure(dJdx, rhs.data(), nf, N, nullptr);  // legacy stream: solve() orders after it
     vg_solve_opts oo = o;
     oo.nonzero_guess = 0;
     solve(rhs.data(), mu.data(), oo, info, s);

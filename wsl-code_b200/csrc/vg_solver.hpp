@@ -50,6 +50,8 @@ public:
     void apply32(const float* x, float* y, bool constrained, float psign, cudaStream_t s, double* quad = nullptr);
     void rhs(double* b, cudaStream_t s);
     void solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_info& info, cudaStream_t s);
+    // host buffers in and out (pinned or pageable); device copies kept across calls
+    void solve_host(const double* b_host, double* x_host, const vg_solve_opts& o, vg_solve_info& info);
     void adjoint(const double* x, const double* dJdx, double* g, const vg_solve_opts& o, vg_solve_info& info,
                  cudaStream_t s);
     void errors(const double* x, double out[6], cudaStream_t s);
@@ -77,6 +79,7 @@ private:
     void pack_streams(cudaStream_t s);
     void check_pipeline();
     void make_diagonal(cudaStream_t s);
+    void lift_flux_rhs();
     void build_amg();
     void check_status(const char* where);
     void axpy64(double* x, const double* d, double a, cudaStream_t s);
@@ -145,6 +148,9 @@ private:
     DevBuf<ApplyBatch> d_bat64_, d_bat32_;
     DevBuf<int> d_cta64_, d_cta32_;
     DevBuf<int> d_err_;
+    DevBuf<double> d_hb_, d_hx_;  // device copies of the host-buffer solve
+    DevBuf<double> d_rhs0_;       // right-hand side before the essential-BC lift
+    DevBuf<double> d_adj_rhs_, d_adj_mu_;  // adjoint right-hand side and solution
 };
 
 }  // namespace vg

@@ -6,6 +6,7 @@
 * ``meshgen``: seeded Voronoi + Lloyd disk / annulus meshes with exact circular-arc boundaries.
 * ``fields``: seeded Gaussian random fields for log permeability.
 * ``autograd``: ``torch.autograd.Function`` over the forward solve and the adjoint gradient.
+* ``observe``: point observations of the pressure (the adjoint's objective).
 """
 from ._lib import VemGpuError, header_functions, lib  # noqa: F401
 from .core import DarcyGpu, DarcySolver, default_nq  # noqa: F401

@@ -149,10 +149,16 @@ class DarcyGpu:
         L.check(L.lib().vg_solve(self.h, b.data_ptr(), x.data_ptr(), ctypes.byref(o), ctypes.byref(info)), self.h)
         return x, dict(iterations=info.iterations, outer=info.outer, residual=info.residual, seconds=info.seconds)
 
-    def solve_host(self, b, **kw):
-        """End-to-end solve from host memory: b (numpy) -> x (numpy)."""
+    def solve_host(self, b, out=None, **kw):
+        """End-to-end solve from host memory: b (numpy) -> x (numpy; `out` if given, e.g. a view of
+        pinned memory)."""
         b = np.ascontiguousarray(b, np.float64)
-        x = np.zeros(self.N)
+        if out is not None:
+            if out.dtype != np.float64 or out.shape != (self.N,) or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous float64 array of length N")
+            x = out
+        else:
+            x = np.zeros(self.N)
         info = L.VgSolveInfo()
         o = self.opts(**kw)
         L.check(L.lib().vg_solve_host(self.h, b.ctypes.data, x.ctypes.data, ctypes.byref(o), ctypes.byref(info)),
