@@ -9,6 +9,8 @@
 // positive definite operator, as MINRES requires of its preconditioner.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <numeric>
 
 #include "vg_amg.hpp"
@@ -459,6 +461,17 @@ void Amg::setup(const HostCsr& S0) {
     }
     std::vector<double> inv = dense_inverse(A);
     ncoarse_ = A.n;
+    if (const char* e = std::getenv("VG_AMG_STATS"); e && *e == '1') {
+        // diagnostics: rows, stored entries and storage of every level (stderr)
+        auto nz = [](const Sell& S) { return (long long)(S.csr ? S.ccol.size() : S.col.size()); };
+        for (size_t l = 0; l < levels_.size(); ++l) {
+            const Level& L = levels_[l];
+            std::fprintf(stderr, "amg level %zu: rows %d A %lld (%s) P %lld (%s) R %lld (%s) omega %.3f\n", l, L.n,
+                         nz(L.A), L.A.csr ? "csr" : "sell", nz(L.P), L.P.csr ? "csr" : "sell", nz(L.R),
+                         L.R.csr ? "csr" : "sell", L.omega);
+        }
+        std::fprintf(stderr, "amg coarsest dense: %d rows\n", ncoarse_);
+    }
     dinvc64_.upload(inv);
     std::vector<float> inv32(inv.begin(), inv.end());
     dinvc32_.upload(inv32);

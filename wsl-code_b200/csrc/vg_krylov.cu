@@ -17,6 +17,42 @@ namespace vg {
 
 namespace {
 
+// 16-byte vector access of 4 consecutive entries (the index is a multiple of 4 and every vector
+// starts on a cudaMalloc boundary): 4 floats in one load, 4 doubles in two
+__device__ __forceinline__ void ld4(const float* p, float (&o)[4]) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+    o[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&o)[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = b.x;
+    o[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// [lo, hi) split into a scalar head up to a multiple of 4, 4-wide body, scalar tail; grid-stride
+template <class F4, class F1>
+__device__ __forceinline__ void for_range(long long lo, long long hi, F4 body4, F1 body1) {
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nth = (long long)gridDim.x * blockDim.x;
+    long long a = (lo + 3) & ~3LL;
+    if (a > hi) a = hi;
+    const long long b = a + ((hi - a) & ~3LL);
+    for (long long i = lo + tid; i < a; i += nth) body1(i);
+    for (long long i = a + 4 * tid; i < b; i += 4 * nth) body4(i);
+    for (long long i = b + tid; i < hi; i += nth) body1(i);
+}
+
 // block + grid reduction of NV values; the last block to finish calls fin(total)
 template <int NV, class F>
 __device__ void grid_reduce(double (&v)[NV], double* partials, unsigned* counter, F fin) {
@@ -117,7 +153,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_init(const T* r, MinresVecs<T> 
                                                       int* flags, double tol, double* partials, unsigned* counter,
                                                       long long plo, long long phi) {
     double acc[1] = {0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    auto one = [&](long long i) {
         T ri = r[i];
         v.v_cur[i] = ri;
         v.v_old[i] = T(0);
@@ -129,7 +165,34 @@ __global__ void __launch_bounds__(VEC_THREADS) k_init(const T* r, MinresVecs<T> 
             v.z_cur[i] = zi;
             acc[0] += double(zi) * double(ri);
         }
-    }
+    };
+    auto four = [&](long long i) {
+        T r4[4], z0[4] = {T(0), T(0), T(0), T(0)};
+        ld4(r + i, r4);
+        st4(v.v_cur + i, r4);
+        st4(v.v_old + i, z0);
+        st4(v.w_cur + i, z0);
+        st4(v.w_old + i, z0);
+        st4(v.y + i, z0);
+        if (i + 3 < plo || i >= phi) {
+            T d4[4], zi[4];
+            ld4(v.dinv + i, d4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                zi[j] = d4[j] * r4[j];
+                acc[0] += double(zi[j]) * double(r4[j]);
+            }
+            st4(v.z_cur + i, zi);
+        } else {
+            for (int j = 0; j < 4; ++j)
+                if (i + j < plo || i + j >= phi) {
+                    T zi = v.dinv[i + j] * r4[j];
+                    v.z_cur[i + j] = zi;
+                    acc[0] += double(zi) * double(r4[j]);
+                }
+        }
+    };
+    for_range(0, n, four, one);
     const bool split = phi > plo;
     grid_reduce<1>(acc, partials, counter, [&](double* tot) {
         if (split)
@@ -150,7 +213,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_update(MinresVecs<T> v, long lo
     const double g = sc->gam, gp = sc->gam_prev, dl = sc->delta / (g * g);
     const T f1 = T(1.0 / g), f2 = T(dl / g), f3 = T(g / gp);
     double acc[1] = {0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    auto one = [&](long long i) {
         T vn = v.y[i] * f1 - f2 * v.v_cur[i] - f3 * v.v_old[i];
         v.v_old[i] = vn;
         v.y[i] = T(0);
@@ -159,7 +222,35 @@ __global__ void __launch_bounds__(VEC_THREADS) k_update(MinresVecs<T> v, long lo
             v.z_new[i] = zn;
             acc[0] += double(zn) * double(vn);
         }
-    }
+    };
+    auto four = [&](long long i) {
+        T y4[4], vc[4], vo[4], vn[4], z0[4] = {T(0), T(0), T(0), T(0)};
+        ld4(v.y + i, y4);
+        ld4(v.v_cur + i, vc);
+        ld4(v.v_old + i, vo);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) vn[j] = y4[j] * f1 - f2 * vc[j] - f3 * vo[j];
+        st4(v.v_old + i, vn);
+        st4(v.y + i, z0);
+        if (i + 3 < plo || i >= phi) {
+            T d4[4], zn[4];
+            ld4(v.dinv + i, d4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                zn[j] = d4[j] * vn[j];
+                acc[0] += double(zn[j]) * double(vn[j]);
+            }
+            st4(v.z_new + i, zn);
+        } else {
+            for (int j = 0; j < 4; ++j)
+                if (i + j < plo || i + j >= phi) {
+                    T zn = v.dinv[i + j] * vn[j];
+                    v.z_new[i + j] = zn;
+                    acc[0] += double(zn) * double(vn[j]);
+                }
+        }
+    };
+    for_range(0, n, four, one);
     const bool split = phi > plo;
     grid_reduce<1>(acc, partials, counter, [&](double* tot) {
         if (split)
@@ -176,9 +267,16 @@ __global__ void __launch_bounds__(VEC_THREADS) k_finish(const T* z, const T* vv,
                                                         int init, double tol) {
     if (!init && flags[0]) return;
     double acc[1] = {0};
-    for (long long i = plo + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < phi;
-         i += (long long)gridDim.x * blockDim.x)
-        acc[0] += double(z[i]) * double(vv[i]);
+    for_range(
+        plo, phi,
+        [&](long long i) {
+            T z4[4], v4[4];
+            ld4(z + i, z4);
+            ld4(vv + i, v4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[0] += double(z4[j]) * double(v4[j]);
+        },
+        [&](long long i) { acc[0] += double(z[i]) * double(vv[i]); });
     grid_reduce<1>(acc, partials, counter, [&](double* tot) {
         double g2 = tot[0] + sc->dot;
         if (init)
@@ -192,11 +290,27 @@ template <typename T>
 __global__ void __launch_bounds__(VEC_THREADS) k_step(MinresVecs<T> v, long long n, Scalars* sc, int* flags) {
     if (!flags[1]) return;
     const T zs = T(sc->zscale), a2 = T(sc->a2), a3 = T(sc->a3), ia1 = T(1.0 / sc->a1), xc = T(sc->xcoef);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        T wn = (v.z_cur[i] * zs - a3 * v.w_old[i] - a2 * v.w_cur[i]) * ia1;
-        v.w_old[i] = wn;
-        v.x[i] += xc * wn;
-    }
+    for_range(
+        0, n,
+        [&](long long i) {
+            T z4[4], wo[4], wc[4], x4[4], wn[4];
+            ld4(v.z_cur + i, z4);
+            ld4(v.w_old + i, wo);
+            ld4(v.w_cur + i, wc);
+            ld4(v.x + i, x4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                wn[j] = (z4[j] * zs - a3 * wo[j] - a2 * wc[j]) * ia1;
+                x4[j] += xc * wn[j];
+            }
+            st4(v.w_old + i, wn);
+            st4(v.x + i, x4);
+        },
+        [&](long long i) {
+            T wn = (v.z_cur[i] * zs - a3 * v.w_old[i] - a2 * v.w_cur[i]) * ia1;
+            v.w_old[i] = wn;
+            v.x[i] += xc * wn;
+        });
 }
 
 // end of one body of the graph's while loop: continue while not converged and below the cap
@@ -242,9 +356,18 @@ __global__ void k_to_float_plain(const double* in, float* out, long long n) {
 
 }  // namespace
 
+// the 4-wide kernels need every vector on a 16-byte boundary (cudaMalloc gives 256)
+template <typename T>
+void check_aligned(const MinresVecs<T>& v, const T* extra = nullptr) {
+    const void* ps[] = {v.v_cur, v.v_old, v.z_cur, v.z_new, v.w_cur, v.w_old, v.y, v.x, v.dinv, extra};
+    for (const void* p : ps)
+        if (reinterpret_cast<uintptr_t>(p) % 16) throw Error(VG_EINVAL, "Krylov vectors must be 16-byte aligned");
+}
+
 template <typename T>
 void minres_init(const T* r, MinresVecs<T> v, long long n, Scalars* sc, int* flags, double tol, double* partials,
                  unsigned* counter, cudaStream_t s, long long plo, long long phi) {
+    check_aligned(v, r);
     k_init<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(r, v, n, sc, flags, tol, partials, counter, plo, phi);
     VG_CUDA(cudaGetLastError());
 }
@@ -252,6 +375,7 @@ void minres_init(const T* r, MinresVecs<T> v, long long n, Scalars* sc, int* fla
 template <typename T>
 void minres_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags, double* partials, unsigned* counter,
                    cudaStream_t s, long long plo, long long phi) {
+    check_aligned(v);
     k_update<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(v, n, sc, flags, partials, counter, plo, phi);
     VG_CUDA(cudaGetLastError());
 }
@@ -259,12 +383,15 @@ void minres_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags, double
 template <typename T>
 void minres_finish(const T* z, const T* v, long long plo, long long phi, Scalars* sc, int* flags, double* partials,
                    unsigned* counter, int init, double tol, cudaStream_t s) {
+    if (reinterpret_cast<uintptr_t>(z) % 16 || reinterpret_cast<uintptr_t>(v) % 16)
+        throw Error(VG_EINVAL, "Krylov vectors must be 16-byte aligned");
     k_finish<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(z, v, plo, phi, sc, flags, partials, counter, init, tol);
     VG_CUDA(cudaGetLastError());
 }
 
 template <typename T>
 void minres_step(MinresVecs<T> v, long long n, Scalars* sc, int* flags, cudaStream_t s) {
+    check_aligned(v);
     k_step<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(v, n, sc, flags);
     VG_CUDA(cudaGetLastError());
 }
