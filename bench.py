@@ -231,6 +231,24 @@ def adjoint_leg(args, rank):
     return out
 
 
+def max_over_ranks(value, dist):
+    """The largest value over all ranks (every rank calls this at the same point); the tensor lives
+    on the GPU for NCCL and on the host for gloo."""
+    if not dist:
+        return float(value)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(seed, rank):
+    """Seed of the permeability field of one replica: replicas solve different fields of the same
+    workload (same mesh, no data exchanged between ranks)."""
+    return seed + 1 + rank
+
+
 def ours(args, rank, world, dist):
     import numpy as np
     import torch
@@ -245,7 +263,7 @@ def ours(args, rank, world, dist):
         dist.barrier()
     mesh, _ = annulus_problem(args.cells, args.seed)
     from vemgpu import fields
-    theta = fields.gaussian_field(fields.cell_centroids(mesh), sigma=2.0, corr=0.1, seed=args.seed + 1 + rank)
+    theta = fields.gaussian_field(fields.cell_centroids(mesh), sigma=2.0, corr=0.1, seed=replica_seed(args.seed, rank))
     t0 = time.time()
     g = vemgpu.DarcyGpu(mesh, k=0, nq=9, ng=9, geometry="arcs", problem="annulus", bc="pressure", theta=theta)
     setup_s = time.time() - t0
@@ -288,10 +306,7 @@ def ours(args, rank, world, dist):
         if dist:
             dist.barrier()
         ms = e0.elapsed_time(e1) / steps
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()), infos, launches
+        return max_over_ranks(ms, dist), infos, launches
 
     clk = ClockSampler(os.path.join(tempfile.gettempdir(), f"vg_clocks_{os.getpid()}.csv"))
     with clk:
@@ -360,11 +375,7 @@ def ours(args, rank, world, dist):
         _, info_h = g.solve_host(bh, out=xh, mode="mixed", tol=1e-10, inner_tol=INNER_TOL)
         if i:
             e2e.append(time.perf_counter() - t)
-    e2e_s = sum(e2e) / len(e2e)
-    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_s = float(t.item())
+    e2e_s = max_over_ranks(sum(e2e) / len(e2e), dist)
     adjoint = None if args.no_adjoint else adjoint_leg(args, rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
@@ -388,6 +399,7 @@ def ours(args, rank, world, dist):
                    "l2": "inputs larger than L2: every MINRES iteration streams the operator (144 MB FP32, "
                          "261 MB FP64) and the multigrid hierarchy; apply timings back to back (operator > L2) "
                          "and with L2 flushed", "parallelism": f"replicas x{world}"},
+        "throughput": {"solves_per_s": world / (ms_mixed * 1e-3), "replicas": world},
         "iterations": info_mixed[0]["iterations"], "outer": info_mixed[0]["outer"],
         "residual": info_mixed[0]["residual"], "setup_s": setup_s, "fp64": res.get("fp64"),
         "kernels": {"apply_fp32_ms": apply32_ms, "apply_fp64_ms": apply64_ms, "apply_fp32_bytes": b32,
@@ -419,7 +431,7 @@ def main():
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
         ours(args, rank, world, dist)
     finally:
