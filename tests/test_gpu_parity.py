@@ -221,3 +221,17 @@ def test_solve_host_matches_device(annulus300):
     xh, info = g.solve_host(b.cpu().numpy())
     assert info["residual"] <= 1e-10
     assert np.array_equal(xd.cpu().numpy(), xh)
+
+
+def test_multigrid_solve_matches_oracle_30k():
+    """k = 0 with the pressure condition at 30,000 cells: a multigrid hierarchy of several levels
+    (30k -> ~3.3k -> dense coarsest) preconditions the pressure block."""
+    m = meshgen.voronoi_mesh(30000, "annulus", seed=61)
+    th = np.random.default_rng(62).normal(0, 1.5, 30000)
+    o, g = pair(m, 0, 9, O.GEOM_ARCS, 0.0, O.PROB_ANNULUS, O.BC_PRESSURE, theta=th)
+    xo, _, _ = o.solve_direct()
+    for mode in ("fp64", "mixed"):
+        x, info = g.solve(tol=1e-10, mode=mode)
+        assert info["residual"] <= 1e-10
+        assert info["iterations"] < 200, info
+        assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)

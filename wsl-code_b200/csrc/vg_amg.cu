@@ -4,7 +4,8 @@
 // three-phase greedy aggregation in row order (rows are cells in Hilbert order, so aggregates are
 // compact); tentative prolongator = aggregate indicator; prolongator smoothed by one damped Jacobi
 // step P = (I - omega D^{-1} A) P_tent with omega = 4 / (3 rho(D^{-1} A)); Galerkin coarse operator
-// R A P with R = P^T; stop at <= 512 rows and invert the coarsest matrix densely.
+// R A P with R = P^T; stop at <= COARSE_MAX rows and invert the coarsest matrix densely on the
+// device (one dense matrix-vector product replaces the levels below).
 // Cycle (device): symmetric V(1,1) cycle with damped Jacobi (same omega) — a fixed symmetric
 // positive definite operator, as MINRES requires of its preconditioner.
 #include <algorithm>
@@ -186,53 +187,19 @@ HostCsr smoothed_prolongator(const HostCsr& A, const std::vector<int>& agg, int 
     return P;
 }
 
-// dense symmetric inverse by Gauss-Jordan with partial pivoting; a tiny diagonal shift keeps a
-// semi-definite coarsest matrix (pure flux boundary: constants in the kernel) invertible
-std::vector<double> dense_inverse(const HostCsr& A) {
-    int n = A.n;
-    std::vector<double> a(size_t(n) * n, 0.0), inv(size_t(n) * n, 0.0);
+// dense copy of the coarsest matrix, row-major; a tiny diagonal shift keeps a semi-definite
+// coarsest matrix (constants in the kernel) invertible
+std::vector<double> dense_of(const HostCsr& A) {
+    const int n = A.n;
+    std::vector<double> a(size_t(n) * n, 0.0);
     double tr = 0;
     for (int i = 0; i < n; ++i)
         for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j) {
             a[size_t(i) * n + A.col[j]] += A.val[j];
             if (A.col[j] == i) tr += A.val[j];
         }
-    for (int i = 0; i < n; ++i) {
-        a[size_t(i) * n + i] += 1e-12 * tr / n;
-        inv[size_t(i) * n + i] = 1.0;
-    }
-    for (int k = 0; k < n; ++k) {
-        int piv = k;
-        for (int i = k + 1; i < n; ++i)
-            if (std::fabs(a[size_t(i) * n + k]) > std::fabs(a[size_t(piv) * n + k])) piv = i;
-        if (piv != k)
-            for (int j = 0; j < n; ++j) {
-                std::swap(a[size_t(k) * n + j], a[size_t(piv) * n + j]);
-                std::swap(inv[size_t(k) * n + j], inv[size_t(piv) * n + j]);
-            }
-        double dk = a[size_t(k) * n + k];
-        if (!(std::fabs(dk) > 0)) throw Error(VG_ESINGULAR, "singular coarsest multigrid matrix");
-        for (int j = 0; j < n; ++j) {
-            a[size_t(k) * n + j] /= dk;
-            inv[size_t(k) * n + j] /= dk;
-        }
-        for (int i = 0; i < n; ++i)
-            if (i != k) {
-                double f = a[size_t(i) * n + k];
-                if (f == 0.0) continue;
-                for (int j = 0; j < n; ++j) {
-                    a[size_t(i) * n + j] -= f * a[size_t(k) * n + j];
-                    inv[size_t(i) * n + j] -= f * inv[size_t(k) * n + j];
-                }
-            }
-    }
-    // symmetrise (the exact inverse is symmetric)
-    for (int i = 0; i < n; ++i)
-        for (int j = i + 1; j < n; ++j) {
-            double v = 0.5 * (inv[size_t(i) * n + j] + inv[size_t(j) * n + i]);
-            inv[size_t(i) * n + j] = inv[size_t(j) * n + i] = v;
-        }
-    return inv;
+    for (int i = 0; i < n; ++i) a[size_t(i) * n + i] += 1e-12 * tr / n;
+    return a;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -371,9 +338,72 @@ __global__ void __launch_bounds__(TPB) k_dense(int n, const T* Ainv, const T* b,
     if (lane == 0) z[row] = acc;
 }
 
+// ---- dense inverse of the (symmetric positive definite) coarsest matrix on the device: in-place
+// Gauss-Jordan without pivoting, one step per pivot k:
+//   a_kk <- 1/p, a_kj <- a_kj/p, a_ik <- -a_ik/p, a_ij <- a_ij - a_ik a_kj / p   (p = a_kk)
+// with column k and row k saved before the step, so every element reads only its own old value
+__global__ void k_gj_save(const double* a, int n, int k, double* col, double* row) {
+    int t = blockIdx.x * TPB + threadIdx.x;
+    if (t < n) {
+        col[t] = a[(long long)t * n + k];
+        row[t] = a[(long long)k * n + t];
+    }
+}
+
+__global__ void k_gj_step(double* a, int n, int k, const double* col, const double* row, unsigned long long* bad) {
+    long long t = blockIdx.x * (long long)TPB + threadIdx.x;
+    if (t >= (long long)n * n) return;
+    const int i = int(t / n), j = int(t % n);
+    const double p = row[k];
+    if (!(p > 0.0)) {  // not positive definite: reported, the result is not used
+        if (t == 0) atomicExch(bad, 1ull);
+        return;
+    }
+    double v;
+    if (i == k && j == k)
+        v = 1.0 / p;
+    else if (i == k)
+        v = row[j] / p;
+    else if (j == k)
+        v = -col[i] / p;
+    else
+        v = a[t] - col[i] * row[j] / p;
+    a[t] = v;
+}
+
+// symmetric part in FP64 and FP32 (the exact inverse is symmetric)
+__global__ void k_gj_sym(const double* a, int n, double* o64, float* o32) {
+    long long t = blockIdx.x * (long long)TPB + threadIdx.x;
+    if (t >= (long long)n * n) return;
+    const int i = int(t / n), j = int(t % n);
+    const double v = 0.5 * (a[t] + a[(long long)j * n + i]);
+    o64[t] = v;
+    o32[t] = float(v);
+}
+
 inline int blocks(int n) { return (n + TPB - 1) / TPB; }
 
 }  // namespace
+
+void Amg::dense_inverse_device(const std::vector<double>& a, int n) {
+    DevBuf<double> d, col(n), row(n);
+    DevBuf<unsigned long long> bad(1);
+    d.upload(a);
+    bad.zero();
+    const long long nn = (long long)n * n;
+    const int nb = int((nn + TPB - 1) / TPB);
+    for (int k = 0; k < n; ++k) {
+        k_gj_save<<<blocks(n), TPB>>>(d.data(), n, k, col.data(), row.data());
+        k_gj_step<<<nb, TPB>>>(d.data(), n, k, col.data(), row.data(), bad.data());
+    }
+    dinvc64_.resize(size_t(nn));
+    dinvc32_.resize(size_t(nn));
+    k_gj_sym<<<nb, TPB>>>(d.data(), n, dinvc64_.data(), dinvc32_.data());
+    VG_CUDA(cudaGetLastError());
+    unsigned long long b = 0;
+    VG_CUDA(cudaMemcpy(&b, bad.data(), sizeof(b), cudaMemcpyDeviceToHost));
+    if (b) throw Error(VG_ESINGULAR, "coarsest multigrid matrix is not positive definite");
+}
 
 long long Amg::nnz() const {
     long long t = 0;
@@ -434,7 +464,7 @@ void Amg::setup(const HostCsr& S0) {
                 }
         };
         to_sell(A, L.A);
-        if (A.n <= 512 || levels_.size() >= 16) {
+        if (A.n <= COARSE_MAX || levels_.size() >= 16) {
             levels_.push_back(std::move(L));
             break;
         }
@@ -459,8 +489,8 @@ void Amg::setup(const HostCsr& S0) {
         levels_.clear();
         throw Error(VG_EINVAL, "multigrid coarsening stalled at " + std::to_string(A.n) + " rows");
     }
-    std::vector<double> inv = dense_inverse(A);
     ncoarse_ = A.n;
+    dense_inverse_device(dense_of(A), A.n);
     if (const char* e = std::getenv("VG_AMG_STATS"); e && *e == '1') {
         // diagnostics: rows, stored entries and storage of every level (stderr)
         auto nz = [](const Sell& S) { return (long long)(S.csr ? S.ccol.size() : S.col.size()); };
@@ -472,9 +502,6 @@ void Amg::setup(const HostCsr& S0) {
         }
         std::fprintf(stderr, "amg coarsest dense: %d rows\n", ncoarse_);
     }
-    dinvc64_.upload(inv);
-    std::vector<float> inv32(inv.begin(), inv.end());
-    dinvc32_.upload(inv32);
     // uploads
     for (auto& L : levels_) {
         auto up = [](const Sell& S, DevBuf<long long>& so, DevBuf<int>& w, DevBuf<int>& c, DevBuf<double>& v64,

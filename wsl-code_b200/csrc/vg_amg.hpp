@@ -40,6 +40,9 @@ struct DevCsr {
     const T* val = nullptr;
 };
 
+// coarsest level: at most this many rows, inverted densely (2500^2 doubles = 50 MB)
+constexpr int COARSE_MAX = 2500;
+
 class Amg {
 public:
     // build the hierarchy of S (host CSR, symmetric positive definite or semi-definite)
@@ -80,6 +83,7 @@ private:
     };
     template <typename T>
     void cycle(int l, const T* b, T* z, cudaStream_t s);
+    void dense_inverse_device(const std::vector<double>& a, int n);
     template <typename T>
     DevSell<T> view(const Level& L, int which) const;
     template <typename T>
