@@ -207,14 +207,35 @@ std::vector<double> dense_of(const HostCsr& A) {
 // ---------------------------------------------------------------------------------------------
 constexpr int TPB = 256;
 
+// one row of a SELL-32 matrix: sum_k val_k xv(col_k), entries loaded four at a time before their
+// gathers (independent loads in flight), fixed summation order
+template <typename T, class X>
+__device__ __forceinline__ T sell_dot(const DevSell<T>& M, int r, X xv) {
+    const int s = r >> 5, l = r & 31;
+    const long long o = __ldg(M.soff + s) + l;
+    const int w = __ldg(M.width + s);
+    const int* cp = M.col + o;
+    const T* vp = M.val + o;
+    T acc = T(0);
+    int k = 0;
+    for (; k + 4 <= w; k += 4) {
+        int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * (k + 1)), c2 = __ldg(cp + 32 * (k + 2)),
+            c3 = __ldg(cp + 32 * (k + 3));
+        T v0 = __ldg(vp + 32 * k), v1 = __ldg(vp + 32 * (k + 1)), v2 = __ldg(vp + 32 * (k + 2)),
+          v3 = __ldg(vp + 32 * (k + 3));
+        T x0 = xv(c0), x1 = xv(c1), x2 = xv(c2), x3 = xv(c3);
+        acc += v0 * x0;
+        acc += v1 * x1;
+        acc += v2 * x2;
+        acc += v3 * x3;
+    }
+    for (; k < w; ++k) acc += __ldg(vp + 32 * k) * xv(__ldg(cp + 32 * k));
+    return acc;
+}
+
 template <typename T>
 __device__ __forceinline__ T sell_row(const DevSell<T>& M, int r, const T* x) {
-    int s = r >> 5, l = r & 31;
-    long long o = M.soff[s] + l;
-    int w = M.width[s];
-    T acc = T(0);
-    for (int k = 0; k < w; ++k) acc += M.val[o + 32LL * k] * x[M.col[o + 32LL * k]];
-    return acc;
+    return sell_dot(M, r, [&](int c) { return x[c]; });
 }
 
 template <typename T>
@@ -229,14 +250,7 @@ __global__ void __launch_bounds__(TPB) k_jacobi0_residual(DevSell<T> A, const T*
                                                           T* r) {
     int i = blockIdx.x * TPB + threadIdx.x;
     if (i >= A.n) return;
-    int s = i >> 5, l = i & 31;
-    long long o = A.soff[s] + l;
-    int w = A.width[s];
-    T acc = T(0);
-    for (int k = 0; k < w; ++k) {
-        int c = A.col[o + 32LL * k];
-        acc += A.val[o + 32LL * k] * (omega * dinv[c] * b[c]);
-    }
+    const T acc = sell_dot(A, i, [&](int c) { return omega * dinv[c] * b[c]; });
     t[i] = omega * dinv[i] * b[i];
     r[i] = b[i] - acc;
 }
@@ -269,7 +283,8 @@ __global__ void __launch_bounds__(TPB) k_smooth(DevSell<T> A, const T* dinv, T o
 template <int G, typename T>
 __device__ __forceinline__ T csr_row(const DevCsr<T>& M, int r, const T* x, int gl) {
     T acc = T(0);
-    for (int j = M.ptr[r] + gl; j < M.ptr[r + 1]; j += G) acc += M.val[j] * x[M.col[j]];
+    const int lo = __ldg(M.ptr + r), hi = __ldg(M.ptr + r + 1);
+    for (int j = lo + gl; j < hi; j += G) acc += __ldg(M.val + j) * x[__ldg(M.col + j)];
 #pragma unroll
     for (int off = G / 2; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off, G);
     return acc;  // valid in lane gl == 0 of the group
@@ -278,9 +293,10 @@ __device__ __forceinline__ T csr_row(const DevCsr<T>& M, int r, const T* x, int 
 template <int G, typename T>
 __device__ __forceinline__ T csr_row_jac(const DevCsr<T>& M, int r, const T* dinv, T omega, const T* b, int gl) {
     T acc = T(0);
-    for (int j = M.ptr[r] + gl; j < M.ptr[r + 1]; j += G) {
-        int c = M.col[j];
-        acc += M.val[j] * (omega * dinv[c] * b[c]);
+    const int lo = __ldg(M.ptr + r), hi = __ldg(M.ptr + r + 1);
+    for (int j = lo + gl; j < hi; j += G) {
+        int c = __ldg(M.col + j);
+        acc += __ldg(M.val + j) * (omega * dinv[c] * b[c]);
     }
 #pragma unroll
     for (int off = G / 2; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off, G);
@@ -320,6 +336,7 @@ void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, 
     long long threads = (long long)M.n * M.group;
     int blocks = int((threads + TPB - 1) / TPB);
     switch (M.group) {
+    case 2: k_csr<2, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
     case 4: k_csr<4, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
     case 8: k_csr<8, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
     case 16: k_csr<16, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
@@ -327,15 +344,30 @@ void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, 
     }
 }
 
-// coarsest level: z = Ainv b, one warp per row
+// coarsest level: z = Ainv b, one block of TPB threads per row (enough warps in flight per SM
+// for a matrix of up to COARSE_MAX^2 entries), fixed-order block reduction
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_dense(int n, const T* Ainv, const T* b, T* z) {
-    int row = (blockIdx.x * TPB + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (row >= n) return;
-    T acc = T(0);
-    for (int j = lane; j < n; j += 32) acc += Ainv[(long long)row * n + j] * b[j];
+    __shared__ T sh[TPB / 32];
+    const int row = blockIdx.x, t = threadIdx.x;
+    const T* a = Ainv + (long long)row * n;
+    T acc0 = T(0), acc1 = T(0);
+    int j = t;
+    for (; j + TPB < n; j += 2 * TPB) {
+        T a0 = __ldcs(a + j), a1 = __ldcs(a + j + TPB);
+        acc0 += a0 * __ldg(b + j);
+        acc1 += a1 * __ldg(b + j + TPB);
+    }
+    if (j < n) acc0 += __ldcs(a + j) * __ldg(b + j);
+    T acc = acc0 + acc1;
     for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-    if (lane == 0) z[row] = acc;
+    if ((t & 31) == 0) sh[t >> 5] = acc;
+    __syncthreads();
+    if (t == 0) {
+        T v = T(0);
+        for (int w = 0; w < TPB / 32; ++w) v += sh[w];
+        z[row] = v;
+    }
 }
 
 // ---- dense inverse of the (symmetric positive definite) coarsest matrix on the device: in-place
@@ -423,12 +455,17 @@ void Amg::setup(const HostCsr& S0) {
             double d = diag_of(A, i);
             L.dinv[i] = d != 0.0 ? 1.0 / d : 0.0;
         }
-        auto to_sell = [](const HostCsr& M, Sell& S) {
+        // storage: SELL-32 (one thread per row) only for the regular fine-level operator; every other
+        // matrix (rectangular P and R, the denser coarse operators) as CSR with a group of lanes per
+        // row sized to about three entries per lane (a power of two in 2..32)
+        auto to_sell = [&](const HostCsr& M, Sell& S, bool sell_ok) {
             S.n = M.n;
             double avg = M.n ? double(M.col.size()) / M.n : 0.0;
-            if (avg > 10.0) {
+            if (!(sell_ok && avg <= 10.0)) {
                 S.csr = true;
-                S.group = avg > 24 ? 32 : avg > 12 ? 16 : 8;
+                int g = 2;
+                while (g < 32 && 3.0 * g * 1.41421356 < avg) g *= 2;
+                S.group = g;
                 S.cptr = M.ptr;
                 S.ccol = M.col;
                 S.cval = M.val;
@@ -463,7 +500,7 @@ void Amg::setup(const HostCsr& S0) {
                     }
                 }
         };
-        to_sell(A, L.A);
+        to_sell(A, L.A, levels_.empty());
         if (A.n <= COARSE_MAX || levels_.size() >= 16) {
             levels_.push_back(std::move(L));
             break;
@@ -479,8 +516,8 @@ void Amg::setup(const HostCsr& S0) {
         HostCsr R = transpose(P);
         HostCsr Ac = spgemm(R, spgemm(A, P));
         L.nc = nagg;
-        to_sell(P, L.P);
-        to_sell(R, L.R);
+        to_sell(P, L.P, false);
+        to_sell(R, L.R, false);
         levels_.push_back(std::move(L));
         A = std::move(Ac);
     }
@@ -583,7 +620,7 @@ void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     if (l == int(levels_.size()) - 1) {
         const T* inv = sizeof(T) == 8 ? reinterpret_cast<const T*>(dinvc64_.data())
                                       : reinterpret_cast<const T*>(dinvc32_.data());
-        k_dense<T><<<(ncoarse_ * 32 + TPB - 1) / TPB, TPB, 0, s>>>(ncoarse_, inv, b, z);
+        k_dense<T><<<ncoarse_, TPB, 0, s>>>(ncoarse_, inv, b, z);
         ++launches;
         return;
     }
