@@ -235,3 +235,17 @@ def test_multigrid_solve_matches_oracle_30k():
         assert info["residual"] <= 1e-10
         assert info["iterations"] < 200, info
         assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+
+
+def test_multigrid_k1_solve_matches_oracle_20k():
+    """k = 1 with the pressure condition at 20,000 cells: the pressure block (three moments per
+    cell) is preconditioned by Jacobi smoothing, injection of the cell means and smoothed
+    aggregation on the mean block."""
+    m = meshgen.voronoi_mesh(20000, "disk", seed=63)
+    o, g = pair(m, 1, 9, O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
+    xo, _, _ = o.solve_direct()
+    for mode in ("fp64", "mixed"):
+        x, info = g.solve(tol=1e-10, mode=mode)
+        assert info["residual"] <= 1e-10
+        assert info["iterations"] < 400, info
+        assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)

@@ -443,7 +443,8 @@ long long Amg::nnz() const {
     return t;
 }
 
-void Amg::setup(const HostCsr& S0) {
+void Amg::setup(const HostCsr& S0, const HostCsr* first_P) {
+    PhaseTimer pt;
     levels_.clear();
     HostCsr A = S0;
     const double theta = 0.08;
@@ -505,14 +506,23 @@ void Amg::setup(const HostCsr& S0) {
             levels_.push_back(std::move(L));
             break;
         }
+        HostCsr P;
         int nagg = 0;
-        std::vector<int> agg = aggregate(A, theta, nagg);
-        if (nagg >= A.n || nagg == 0) {  // no coarsening possible
-            levels_.push_back(std::move(L));
-            break;
+        if (levels_.empty() && first_P) {
+            if (first_P->n != A.n || first_P->m <= 0 || first_P->m >= A.n)
+                throw Error(VG_EINVAL, "first multigrid prolongator does not fit the matrix");
+            L.omega = 4.0 / (3.0 * rho_dinv_a(A, L.dinv));
+            P = *first_P;
+            nagg = P.m;
+        } else {
+            std::vector<int> agg = aggregate(A, theta, nagg);
+            if (nagg >= A.n || nagg == 0) {  // no coarsening possible
+                levels_.push_back(std::move(L));
+                break;
+            }
+            L.omega = 4.0 / (3.0 * rho_dinv_a(A, L.dinv));
+            P = smoothed_prolongator(A, agg, nagg, L.dinv, L.omega);
         }
-        L.omega = 4.0 / (3.0 * rho_dinv_a(A, L.dinv));
-        HostCsr P = smoothed_prolongator(A, agg, nagg, L.dinv, L.omega);
         HostCsr R = transpose(P);
         HostCsr Ac = spgemm(R, spgemm(A, P));
         L.nc = nagg;
@@ -520,6 +530,7 @@ void Amg::setup(const HostCsr& S0) {
         to_sell(R, L.R, false);
         levels_.push_back(std::move(L));
         A = std::move(Ac);
+        pt.mark("multigrid level (host)");
     }
     // coarsest level: dense inverse (bounded size; otherwise the caller keeps its diagonal preconditioner)
     if (A.n > 4096) {
@@ -528,7 +539,8 @@ void Amg::setup(const HostCsr& S0) {
     }
     ncoarse_ = A.n;
     dense_inverse_device(dense_of(A), A.n);
-    if (const char* e = std::getenv("VG_AMG_STATS"); e && *e == '1') {
+    pt.mark("coarsest dense inverse");
+    if (PhaseTimer::stats_enabled()) {
         // diagnostics: rows, stored entries and storage of every level (stderr)
         auto nz = [](const Sell& S) { return (long long)(S.csr ? S.ccol.size() : S.col.size()); };
         for (size_t l = 0; l < levels_.size(); ++l) {
@@ -571,6 +583,7 @@ void Amg::setup(const HostCsr& S0) {
         for (auto* b : {&L.x64, &L.b64, &L.r64, &L.t64}) b->resize(L.n);
         for (auto* b : {&L.x32, &L.b32, &L.r32, &L.t32}) b->resize(L.n);
     }
+    pt.mark("multigrid uploads");
 }
 
 template <typename T>

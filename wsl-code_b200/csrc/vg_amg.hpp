@@ -45,8 +45,9 @@ constexpr int COARSE_MAX = 2500;
 
 class Amg {
 public:
-    // build the hierarchy of S (host CSR, symmetric positive definite or semi-definite)
-    void setup(const HostCsr& S);
+    // build the hierarchy of S (host CSR, symmetric positive definite or semi-definite); first_P, when
+    // given, is the prolongator of the finest level (no aggregation there)
+    void setup(const HostCsr& S, const HostCsr* first_P);
     bool ready() const { return !levels_.empty(); }
     int levels() const { return int(levels_.size()); }
     long long nnz() const;

@@ -68,7 +68,9 @@ int vg_create_polygons(int num_nodes, const double* node_coords, int num_cells, 
     *out = nullptr;
     try {
         vg::HostMesh m;
+        vg::PhaseTimer pt;
         vg::process_polygons(m, num_nodes, node_coords, num_cells, cell_ptr, cell_nodes);
+        pt.mark("reader post-processing");
         return create(std::move(m), geometry, k, nq, ng, device, out);
     } catch (const vg::Error& e) {
         g_create_error = e.what();

@@ -8,6 +8,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <ctime>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -83,6 +86,28 @@ public:
     T* data() { return p_; }
     const T* data() const { return p_; }
     size_t size() const { return n_; }
+};
+
+// diagnostics: wall time of setup phases on stderr when the environment sets VG_STATS=1
+struct PhaseTimer {
+    bool on;
+    double t;
+    static double now() {
+        timespec ts;
+        clock_gettime(CLOCK_MONOTONIC, &ts);
+        return ts.tv_sec + 1e-9 * ts.tv_nsec;
+    }
+    PhaseTimer() : on(stats_enabled()), t(now()) {}
+    static bool stats_enabled() {
+        const char* e = std::getenv("VG_STATS");
+        return e && *e == '1';
+    }
+    void mark(const char* what) {
+        if (!on) return;
+        const double n = now();
+        std::fprintf(stderr, "vg setup %-28s %8.3f s\n", what, n - t);
+        t = n;
+    }
 };
 
 // ---------------------------------------------------------------------------------------------

@@ -231,8 +231,11 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
                 if (edge_arc[m.gedges[j]] >= 0) curved[c] = 1;
     std::vector<int> triptr;
     std::vector<TriIdx> tris;
+    PhaseTimer pt;
     triangulate(m, curved, edge_arc, triptr, tris);
+    pt.mark("triangulate");
     pack_layout();
+    pt.mark("pack layout");
     // uploads
     d_xy_.upload(m.xy);
     d_cptr_.upload(m.cptr);
@@ -248,7 +251,9 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
     d_cell_slot_.upload(cell_slot_);
     d_pieces_.upload(pieces_);
     d_map_.upload(map_host_);
+    pt.mark("uploads");
     plan_streams();
+    pt.mark("record-stream plan");
     {
         std::vector<int> occ(m.eocc);
         DevBuf<int> tmp;
@@ -455,10 +460,13 @@ void Solver::build() {
     a.mask = d_mask_.data();
     a.status = d_status_.data();
     setup_args_ = a;
+    PhaseTimer pt;
     for (const auto& c : classes_) launch_setup(a, c, nqp, nullptr);
     VG_CUDA(cudaDeviceSynchronize());
     check_status("setup");
+    pt.mark("device setup kernels");
     pack_streams(nullptr);
+    pt.mark("pack record streams");
     // workspaces
     d_partials_.resize(2 * size_t(std::max(apply_blocks(int(pieces_.size())), VEC_BLOCKS)) + 16);
     d_red_.resize(8);
@@ -474,6 +482,7 @@ void Solver::build() {
     for (auto& b : sv64_) b.resize(N);
     for (auto& b : sv32_) b.resize(N);
     make_diagonal(nullptr);
+    pt.mark("preconditioner (incl. multigrid)");
     // BC_FLUX: lifted right-hand side of MixedGpu::make_rhs (equation_gpu.cu:611-625):
     // free rows b - A g (unconstrained apply of the boundary values), boundary rows g
     d_rhs0_.resize(N);
@@ -512,12 +521,124 @@ void Solver::make_diagonal(cudaStream_t s) {
     // below frees: drop them (they are captured again by the next solve)
     destroy_graphs();
     use_amg = false;
-    if (k == 0 && bc == VG_BC_PRESSURE) build_amg();
+    if (bc == VG_BC_PRESSURE) build_amg();
+}
+
+// pressure Schur block S = B diag(A)^{-1} B^T for k >= 1 (B[(E,r), g] = W_E[r,i] s_Ei over the local
+// flux dofs i of E with global index g and orientation sign s): q x q blocks between cells that share
+// an edge. Its multigrid starts with an injection of the cell means (the m_0 moment) onto the cell
+// graph, where the mean-mean block is coarsened by smoothed aggregation as for k = 0.
+void Solver::build_amg_high() {
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<double> dinv(nf);
+    VG_CUDA(cudaMemcpy(dinv.data(), d_dinv64_.data(), sizeof(double) * nf, cudaMemcpyDeviceToHost));
+    std::vector<double> W = d_W64_.download();
+    // incidences of every flux dof: (cell, local dof, sign), at most two per dof
+    struct Inc {
+        int cell, i;
+        double s;
+    };
+    std::vector<int> cnt(nf + 1, 0);
+    for (int c = 0; c < m.nc; ++c) {
+        const int slot = cell_slot_[c];
+        const Piece& P = pieces_[slot / PIECE];
+        const int lane = slot % PIECE;
+        for (int i = 0; i < P.n; ++i) {
+            int g = map_host_[P.map_off + (long long)i * PIECE + lane];
+            cnt[(g < 0 ? ~g : g) + 1]++;
+        }
+    }
+    for (int g = 0; g < nf; ++g) cnt[g + 1] += cnt[g];
+    std::vector<Inc> inc(cnt[nf]);
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (int c = 0; c < m.nc; ++c) {
+        const int slot = cell_slot_[c];
+        const Piece& P = pieces_[slot / PIECE];
+        const int lane = slot % PIECE;
+        for (int i = 0; i < P.n; ++i) {
+            int g = map_host_[P.map_off + (long long)i * PIECE + lane];
+            int gg = g < 0 ? ~g : g;
+            inc[fill[gg]++] = Inc{c, i, g < 0 ? -1.0 : 1.0};
+        }
+    }
+    auto wv = [&](int c, int r, int i) {
+        const int slot = cell_slot_[c];
+        const Piece& P = pieces_[slot / PIECE];
+        return W[P.w_off + (long long)(r * P.n + i) * PIECE + slot % PIECE];
+    };
+    const int np_ = m.nc * q;
+    // row by row with one sparse accumulator: row (E, r) couples to (F, r2) through every flux dof
+    // shared by E and F
+    HostCsr S;
+    S.n = S.m = np_;
+    S.ptr.assign(np_ + 1, 0);
+    std::vector<double> acc(np_, 0.0);
+    std::vector<int> mark(np_, -1), cols;
+    for (int c = 0; c < m.nc; ++c) {
+        const int slot = cell_slot_[c];
+        const Piece& P = pieces_[slot / PIECE];
+        const int lane = slot % PIECE;
+        for (int r = 0; r < q; ++r) {
+            const int row = c * q + r;
+            cols.clear();
+            for (int i = 0; i < P.n; ++i) {
+                const int g0 = map_host_[P.map_off + (long long)i * PIECE + lane];
+                const int g = g0 < 0 ? ~g0 : g0;
+                const double coef = wv(c, r, i) * (g0 < 0 ? -1.0 : 1.0) * dinv[g];
+                if (coef == 0.0) continue;
+                for (int b = cnt[g]; b < cnt[g + 1]; ++b) {
+                    const Inc& B = inc[b];
+                    for (int r2 = 0; r2 < q; ++r2) {
+                        const int col = B.cell * q + r2;
+                        if (mark[col] != row) {
+                            mark[col] = row;
+                            acc[col] = 0.0;
+                            cols.push_back(col);
+                        }
+                        acc[col] += coef * wv(B.cell, r2, B.i) * B.s;
+                    }
+                }
+            }
+            std::sort(cols.begin(), cols.end());
+            for (int col : cols) {
+                S.col.push_back(col);
+                S.val.push_back(acc[col]);
+            }
+            S.ptr[row + 1] = int(S.col.size());
+        }
+    }
+    // injection of the cell means: pressure row (E, 0) -> coarse E
+    HostCsr P0;
+    P0.n = np_;
+    P0.m = m.nc;
+    P0.ptr.assign(np_ + 1, 0);
+    for (int c = 0; c < m.nc; ++c)
+        for (int r = 0; r < q; ++r) {
+            if (r == 0) {
+                P0.col.push_back(c);
+                P0.val.push_back(1.0);
+            }
+            P0.ptr[c * q + r + 1] = int(P0.col.size());
+        }
+    try {
+        amg_.setup(S, &P0);
+    } catch (const Error&) {
+        use_amg = false;
+        amg_levels = 0;
+        return;
+    }
+    amg_levels = amg_.levels();
+    use_amg = true;
+    amg_setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // pressure Schur block S = W diag(A)^{-1} W^T of the k = 0 system (cell graph: S_EE = sum over the
 // edges of E of 1/d_e, S_EF = -1/d_e across the shared edge e) and its multigrid hierarchy
 void Solver::build_amg() {
+    if (k >= 1) {
+        build_amg_high();
+        return;
+    }
     auto t0 = std::chrono::steady_clock::now();
     std::vector<double> dinv(nf);
     VG_CUDA(cudaMemcpy(dinv.data(), d_dinv64_.data(), sizeof(double) * nf, cudaMemcpyDeviceToHost));
@@ -557,7 +678,7 @@ void Solver::build_amg() {
         S.ptr[c + 1] = int(S.col.size());
     }
     try {
-        amg_.setup(S);
+        amg_.setup(S, nullptr);
     } catch (const Error&) {
         use_amg = false;  // diagonal preconditioner on the device
         amg_levels = 0;

@@ -81,6 +81,7 @@ private:
     void make_diagonal(cudaStream_t s);
     void lift_flux_rhs();
     void build_amg();
+    void build_amg_high();
     void check_status(const char* where);
     void axpy64(double* x, const double* d, double a, cudaStream_t s);
     void minres(bool fp32, const void* b, void* x, double tol, int maxit, int check_every, int& iters,
