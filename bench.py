@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--profile", action="store_true", help="short fixed run for profilers (applies + 2 solves)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient workload")
     ap.add_argument("--adjoint-cells", type=int, default=250000)
+    ap.add_argument("--fd-directions", type=int, default=20)
+    ap.add_argument("--no-config1", action="store_true", help="skip the 250k-cell disk k=0/k=1 leg")
+    ap.add_argument("--config1-cells", type=int, default=250000)
     ap.add_argument("--eager", action="store_true", help="with --profile: host-driven Krylov batches, no graph")
     return ap.parse_args()
 
@@ -67,6 +70,23 @@ def traffic_bytes(kernel, cells):
         return t["bytes"] * cells / t["cells"]
     except Exception:
         return None
+
+
+def disk_mesh(cells, seed):
+    """Voronoi + Lloyd mesh of the unit disk with exact arcs (cached on disk)."""
+    import numpy as np
+    from vemgpu import meshgen
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"disk_{cells}_s{seed}.npz")
+    if os.path.exists(path):
+        z = np.load(path)
+        return {k: z[k] for k in z.files}
+    mesh = meshgen.voronoi_mesh(cells, "disk", seed=seed)
+    mesh = {k: v for k, v in mesh.items() if isinstance(v, np.ndarray)}
+    tmp = path + f".{os.getpid()}.tmp.npz"
+    np.savez(tmp, **mesh)
+    os.replace(tmp, path)
+    return mesh
 
 
 def annulus_problem(cells, seed):
@@ -176,10 +196,11 @@ def reference_arm(args, rank):
 
 
 def adjoint_leg(args, rank):
-    """Gradient workload: 250k-cell annulus, lognormal K, J = sum over 64 seeded interior points
-    of (p_h - d)^2. Reports the adjoint (vg_adjoint_grad: adjoint solve + per-cell contraction)
-    against the forward solve, both device-timed, and central differences (step 1e-6) of J along two
-    seeded unit directions against the adjoint's directional derivative."""
+    """Gradient workload (250k-cell annulus, lognormal K): J = sum over 64 seeded interior points of
+    (p_h - d)^2, the data d being the pressures of a solve with a second seeded K field. Reports the
+    adjoint (vg_adjoint_grad: adjoint solve + per-cell contraction) against the forward solve, both
+    device-timed, and FP64 central differences (step 1e-6, solves to 1e-12) of J along 20 seeded unit
+    directions against the adjoint's directional derivatives."""
     import numpy as np
     import torch
     import vemgpu
@@ -187,17 +208,20 @@ def adjoint_leg(args, rank):
     from vemgpu.autograd import darcy_solve
     cells = args.adjoint_cells
     mesh, _ = annulus_problem(cells, args.seed)
-    th = fields.gaussian_field(fields.cell_centroids(mesh), sigma=2.0, corr=0.1, seed=args.seed + 11 + rank)
-    h = vemgpu.DarcyGpu(mesh, k=0, nq=9, ng=9, geometry="arcs", problem="annulus", bc="pressure", theta=th)
-    obs = observe.PointObservation(h, mesh, observe.seeded_points(64, args.seed + 12),
-                                   data=np.random.default_rng(args.seed + 13).uniform(0.2, 0.8, 64))
-    out = {"cells": h.nc, "observations": 64}
+    cen = fields.cell_centroids(mesh)
+    th = fields.gaussian_field(cen, sigma=2.0, corr=0.1, seed=args.seed + 11 + rank)
+    th_data = fields.gaussian_field(cen, sigma=2.0, corr=0.1, seed=args.seed + 21 + rank)
+    h = vemgpu.DarcyGpu(mesh, k=0, nq=9, ng=9, geometry="arcs", problem="annulus", bc="pressure", theta=th_data)
+    obs = observe.PointObservation(h, mesh, observe.seeded_points(64, args.seed + 12))
+    xd, _ = h.solve(tol=1e-12)
+    obs.data = obs.pressure(xd).clone()
+    h.set_log_permeability(th)
+    out = {"cells": h.nc, "observations": 64, "data": "pressures of a second seeded K field"}
     for mode in ("mixed", "fp64"):
         opts = dict(mode=mode, tol=1e-10, inner_tol=INNER_TOL)
         fw, ad = [], []
         for i in range(4):
             x, info = h.solve(**opts)
-            J = obs(x)
             dJdx = torch.autograd.functional.vjp(obs, x)[1]
             g, ainfo = h.adjoint_grad(x, dJdx, **opts)
             if i:
@@ -207,27 +231,50 @@ def adjoint_leg(args, rank):
         out[mode] = {"forward_s": float(np.mean(fw)), "adjoint_s": float(np.mean(ad)),
                      "grad_over_solve": float(np.mean(ad) / np.mean(fw)),
                      "forward_iterations": info["iterations"], "adjoint_iterations": ainfo["iterations"]}
-    # central differences of J (FP64 solves to 1e-12) against the adjoint directional derivative
     theta = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
     J = obs(darcy_solve(h, theta, tol=1e-12))
     J.backward()
-    rng = np.random.default_rng(args.seed + 14)
     gn = float(torch.linalg.norm(theta.grad))
-    fd = []
+    rng = np.random.default_rng(args.seed + 14)
+    ad, fd = [], []
+    t0 = time.time()
     with torch.no_grad():
-        # the gradient direction (derivative = |g|) and one seeded random unit direction
-        for name, v in (("gradient", theta.grad / gn),
-                        ("random", torch.tensor(rng.standard_normal(h.nc), device="cuda"))):
+        for _ in range(args.fd_directions):
+            v = torch.tensor(rng.standard_normal(h.nc), device="cuda")
             v = v / torch.linalg.norm(v)
             jp = float(obs(darcy_solve(h, theta + 1e-6 * v, tol=1e-12)))
             jm = float(obs(darcy_solve(h, theta - 1e-6 * v, tol=1e-12)))
-            dd, cd = float(theta.grad @ v), (jp - jm) / 2e-6
-            fd.append({"direction": name, "adjoint": dd, "central_difference": cd,
-                       "diff_over_grad_norm": abs(dd - cd) / gn})
-    out["fd_check"] = fd
+            ad.append(float(theta.grad @ v))
+            fd.append((jp - jm) / 2e-6)
+    ad, fd = np.array(ad), np.array(fd)
+    out["fd_check"] = {"directions": len(ad), "step": 1e-6,
+                       "max_abs_diff_over_max_abs_derivative": float(np.abs(ad - fd).max() / np.abs(ad).max()),
+                       "max_abs_diff_over_grad_norm": float(np.abs(ad - fd).max() / gn),
+                       "seconds": time.time() - t0}
     out["grad_norm"] = gn
     out["J"] = float(J.detach())
     h.close()
+    return out
+
+
+def config1_leg(args):
+    """Disk problem of the reference's own examples at 250k cells: p = sin(pi x) sin(pi y), Dirichlet
+    pressure, K = I, k = 0 and k = 1, FP64 and mixed solves to 1e-10 (device time) and the L2 errors
+    against the manufactured solution."""
+    import vemgpu
+    mesh = disk_mesh(args.config1_cells, args.seed)
+    out = {"cells": len(mesh["cell_ptr"]) - 1}
+    for k in (0, 1):
+        g = vemgpu.DarcyGpu(mesh, k=k, geometry="arcs", problem="sinsin", bc="pressure")
+        row = {"dofs": g.N}
+        for mode in ("fp64", "mixed"):
+            g.solve(tol=1e-10, mode=mode, inner_tol=INNER_TOL)
+            x, info = g.solve(tol=1e-10, mode=mode, inner_tol=INNER_TOL)
+            row[mode] = {"solve_s": info["seconds"], "iterations": info["iterations"], "residual": info["residual"]}
+        e = g.errors(x)
+        row["l2_pressure"], row["l2_flux"] = e["scalar_phys"], e["flux_phys"]
+        out[f"k{k}"] = row
+        g.close()
     return out
 
 
@@ -377,6 +424,7 @@ def ours(args, rank, world, dist):
             e2e.append(time.perf_counter() - t)
     e2e_s = max_over_ranks(sum(e2e) / len(e2e), dist)
     adjoint = None if args.no_adjoint else adjoint_leg(args, rank)
+    config1 = None if args.no_config1 else config1_leg(args)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
         threads = 1
@@ -412,6 +460,7 @@ def ours(args, rank, world, dist):
                      "fp64_traffic": traffic_bytes("apply_bulk_kernel<double, 0>", g.nc)},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * g.N, "d2h_bytes_per_step": 8 * g.N},
         "adjoint": adjoint,
+        "disk_250k": config1,
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
