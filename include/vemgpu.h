@@ -121,6 +121,12 @@ int vg_create_polygons(int num_nodes, const double* node_coords, int num_cells, 
                        const int* cell_nodes, const vg_geometry* geometry, int k, int nq, int ng, int device,
                        vg_handle** out);
 
+/* Legacy ASCII VTK polygon file (POINTS, CELLS with a vertex count per cell, CELL_TYPES 5/7/9; other
+ * sections skipped), then the same post-processing as vg_create_polygons. Replaces
+ * StraightMeshReader::read_mesh_vtk (vem/CurvedVEM_Darcy_gpu/mesh/straight_mesh.h:101,
+ * straight_mesh.cpp:68-218) followed by the handle construction. Arcs, if any, come in geometry. */
+int vg_create_vtk(const char* path, const vg_geometry* geometry, int k, int nq, int ng, int device, vg_handle** out);
+
 int vg_destroy(vg_handle* h);
 const char* vg_last_error(const vg_handle* h);
 

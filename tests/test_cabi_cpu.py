@@ -104,3 +104,21 @@ def test_default_options(L):
     o = L.VgSolveOpts()
     L.lib().vg_default_solve_opts(ctypes.byref(o))
     assert o.mode == L.SOLVE_FP64 and o.tol == 1e-10 and o.check_every == 0 and 0 < o.inner_tol < 1
+
+
+def test_vtk_reader_errors_before_device_work(L, tmp_path):
+    """vg_create_vtk parses and checks the file on the host before any device call."""
+    h = ctypes.c_void_p()
+    g = L.VgGeometry()
+    code = L.lib().vg_create_vtk(str(tmp_path / "missing.vtk").encode(), ctypes.byref(g), 1, 9, 9, -1, ctypes.byref(h))
+    assert code == L.VG_EINVAL and b"cannot open" in L.lib().vg_last_error(None)
+    p = tmp_path / "bad.vtk"
+    p.write_text("# vtk DataFile Version 2.0\nx\nASCII\nDATASET UNSTRUCTURED_GRID\nPOINTS 3 float\n0 0 0 1 0 0 0 1 0\n"
+                 "CELLS 1 4\n3 0 1 2\nCELL_TYPES 1\n12\n")
+    code = L.lib().vg_create_vtk(str(p).encode(), ctypes.byref(g), 1, 9, 9, -1, ctypes.byref(h))
+    assert code == L.VG_EMESH and b"unsupported type" in L.lib().vg_last_error(None)
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        p.write_text(p.read_text().replace("\n12\n", "\n5\n"))
+        code = L.lib().vg_create_vtk(str(p).encode(), ctypes.byref(g), 1, 9, 9, -1, ctypes.byref(h))
+        assert code == L.VG_ECUDA

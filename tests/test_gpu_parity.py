@@ -249,3 +249,17 @@ def test_multigrid_k1_solve_matches_oracle_20k():
         assert info["residual"] <= 1e-10
         assert info["iterations"] < 400, info
         assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+
+
+def test_vtk_file_handle_matches_dict_handle(tmp_path, disk200):
+    """vg_create_vtk (C++ reader of the legacy VTK polygon file) builds the same operator as the
+    raw-polygon entry point."""
+    from vemgpu import meshio
+    p = tmp_path / "disk.vtk"
+    meshio.write_vtk(p, disk200)
+    a = vemgpu.DarcyGpu(str(p), k=1, geometry="arcs", problem="sinsin", bc="pressure")
+    b = vemgpu.DarcyGpu(disk200, k=1, geometry="arcs", problem="sinsin", bc="pressure")
+    assert (a.nc, a.ne, a.N) == (b.nc, b.ne, b.N)
+    x = torch.randn(a.N, dtype=torch.float64, device="cuda")
+    assert torch.equal(a.apply(x), b.apply(x))
+    assert torch.equal(a.rhs(), b.rhs())

@@ -81,6 +81,25 @@ int vg_create_polygons(int num_nodes, const double* node_coords, int num_cells, 
     }
 }
 
+int vg_create_vtk(const char* path, const vg_geometry* geometry, int k, int nq, int ng, int device, vg_handle** out) {
+    if (!out) return VG_EINVAL;
+    *out = nullptr;
+    try {
+        std::vector<double> xy;
+        std::vector<int> ptr, nodes;
+        vg::read_vtk_polygons(path, xy, ptr, nodes);
+        vg::HostMesh m;
+        vg::process_polygons(m, int(xy.size() / 2), xy.data(), int(ptr.size()) - 1, ptr.data(), nodes.data());
+        return create(std::move(m), geometry, k, nq, ng, device, out);
+    } catch (const vg::Error& e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return VG_EINVAL;
+    }
+}
+
 int vg_destroy(vg_handle* h) {
     delete h;
     return VG_OK;

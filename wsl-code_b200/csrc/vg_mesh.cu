@@ -12,11 +12,68 @@
 //     the fan of one triangle per edge from the vertex average instead.
 #include <algorithm>
 #include <cmath>
+#include <fstream>
 #include <numeric>
+#include <string>
 
 #include "vg_solver.hpp"
 
 namespace vg {
+
+// Legacy ASCII VTK polygon mesh, the format of the reference reader's VTK path
+// (vem/CurvedVEM_Darcy_gpu/mesh/straight_mesh.cpp:96-218): free-format tokens; POINTS n <type> with
+// three coordinates per point (z dropped); CELLS m <total> with a vertex count before each cell's
+// vertices; CELL_TYPES m with types 5 (triangle), 7 (polygon) or 9 (quad). Other sections (FIELD,
+// CELL_DATA, ...) are skipped. Vertex order is normalised later by process_polygons.
+void read_vtk_polygons(const char* path, std::vector<double>& xy, std::vector<int>& ptr, std::vector<int>& nodes) {
+    if (!path) throw Error(VG_EINVAL, "null path");
+    std::ifstream in(path);
+    if (!in) throw Error(VG_EINVAL, std::string("cannot open ") + path);
+    auto seek = [&](const char* key) {
+        std::string tok;
+        while (in >> tok)
+            if (tok == key) return true;
+        return false;
+    };
+    if (!seek("POINTS")) throw Error(VG_EMESH, "VTK: POINTS section not found");
+    long long nn = 0;
+    std::string type;
+    if (!(in >> nn >> type) || nn <= 0 || nn > (1LL << 31) - 1) throw Error(VG_EMESH, "VTK: invalid POINTS header");
+    xy.assign(2 * size_t(nn), 0.0);
+    for (long long i = 0; i < nn; ++i) {
+        double x, y, z;
+        if (!(in >> x >> y >> z)) throw Error(VG_EMESH, "VTK: failed to read point " + std::to_string(i));
+        xy[2 * i] = x;
+        xy[2 * i + 1] = y;
+    }
+    if (!seek("CELLS")) throw Error(VG_EMESH, "VTK: CELLS section not found");
+    long long nc = 0, total = 0;
+    if (!(in >> nc >> total) || nc <= 0 || nc > (1LL << 31) - 1) throw Error(VG_EMESH, "VTK: invalid CELLS header");
+    ptr.assign(1, 0);
+    nodes.clear();
+    nodes.reserve(size_t(std::max(0LL, total - nc)));
+    for (long long e = 0; e < nc; ++e) {
+        int nv = 0;
+        if (!(in >> nv)) throw Error(VG_EMESH, "VTK: failed to read the vertex count of cell " + std::to_string(e));
+        if (nv < 3) throw Error(VG_EMESH, "VTK: cell " + std::to_string(e) + " has fewer than 3 vertices");
+        for (int i = 0; i < nv; ++i) {
+            long long v = -1;
+            if (!(in >> v)) throw Error(VG_EMESH, "VTK: failed to read a vertex of cell " + std::to_string(e));
+            if (v < 0 || v >= nn) throw Error(VG_EMESH, "VTK: cell " + std::to_string(e) + " references a node out of range");
+            nodes.push_back(int(v));
+        }
+        ptr.push_back(int(nodes.size()));
+    }
+    if (!seek("CELL_TYPES")) throw Error(VG_EMESH, "VTK: CELL_TYPES section not found");
+    long long nt = 0;
+    if (!(in >> nt) || nt != nc) throw Error(VG_EMESH, "VTK: CELL_TYPES count does not match CELLS");
+    for (long long e = 0; e < nc; ++e) {
+        int t = 0;
+        if (!(in >> t)) throw Error(VG_EMESH, "VTK: failed to read cell type " + std::to_string(e));
+        if (t != 5 && t != 7 && t != 9)
+            throw Error(VG_EMESH, "VTK: cell " + std::to_string(e) + " has unsupported type " + std::to_string(t));
+    }
+}
 
 void process_polygons(HostMesh& m, int nn, const double* xy, int nc, const int* ptr, const int* nodes) {
     if (nn <= 0 || nc <= 0 || !xy || !ptr || !nodes) throw Error(VG_EINVAL, "empty mesh");

@@ -28,6 +28,8 @@ struct HostMesh {
 
 // reader post-processing of raw polygons (straight_mesh.cpp:467-664)
 void process_polygons(HostMesh& m, int nn, const double* xy, int nc, const int* ptr, const int* nodes);
+// legacy ASCII VTK polygon file (POINTS / CELLS / CELL_TYPES) -> raw polygons
+void read_vtk_polygons(const char* path, std::vector<double>& xy, std::vector<int>& ptr, std::vector<int>& nodes);
 // copy and validate an already processed mesh
 void copy_processed(HostMesh& m, const vg_mesh& in);
 // triangulation: reference ear clipping (decisions in cell-scaled coordinates) or, for cells with

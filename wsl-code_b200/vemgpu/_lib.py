@@ -59,6 +59,7 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         L.vg_create.argtypes = [ctypes.POINTER(VgMesh), ctypes.POINTER(VgGeometry), I, I, I, I, ctypes.POINTER(P)]
         L.vg_create_polygons.argtypes = [I, P, I, P, P, ctypes.POINTER(VgGeometry), I, I, I, I, ctypes.POINTER(P)]
+        L.vg_create_vtk.argtypes = [ctypes.c_char_p, ctypes.POINTER(VgGeometry), I, I, I, I, ctypes.POINTER(P)]
         L.vg_destroy.argtypes = [P]
         L.vg_last_error.argtypes = [P]
         L.vg_last_error.restype = ctypes.c_char_p

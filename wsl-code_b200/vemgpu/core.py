@@ -29,7 +29,8 @@ def _torch():
 
 
 class DarcyGpu:
-    """One solver handle. mesh: dict with raw polygons (xy, cell_ptr, cell_nodes) or the processed
+    """One solver handle. mesh: path of a legacy VTK polygon file (vemgpu.meshio), dict with raw
+    polygons (xy, cell_ptr, cell_nodes) or the processed
     reader arrays (node_coords, cell_nodes, cell_node_indices, global_edges, edge_endpoints,
     edge_occurrence, cell_centroid_x, cell_centroid_y, cell_diameter); optional arc_nodes /
     arc_data for circular boundary arcs. geometry: 'identity', 'sine' (eps) or 'arcs'."""
@@ -38,6 +39,13 @@ class DarcyGpu:
                  theta=None, device=-1, build=True):
         self._keep = []
         lib = L.lib()
+        vtk_path = None
+        if isinstance(mesh, (str, bytes)) or hasattr(mesh, "__fspath__"):
+            # legacy VTK polygon file, read by the C ABI (vg_create_vtk); arcs from its FIELD block
+            import os
+            from . import meshio
+            vtk_path = os.fsencode(mesh)
+            mesh = meshio.read_vtk_arcs(mesh)
         nq = default_nq(k) if nq is None else nq
         g = L.VgGeometry()
         g.kind = L.GEOM[geometry]
@@ -51,7 +59,9 @@ class DarcyGpu:
             g.arc_nodes = an.ctypes.data
             g.arc_circles = ad.ctypes.data
         h = ctypes.c_void_p()
-        if "xy" in mesh:
+        if vtk_path is not None:
+            code = lib.vg_create_vtk(vtk_path, ctypes.byref(g), k, nq, ng, device, ctypes.byref(h))
+        elif "xy" in mesh:
             xy = np.ascontiguousarray(mesh["xy"], np.float64).reshape(-1)
             ptr = np.ascontiguousarray(mesh["cell_ptr"], np.int32)
             nodes = np.ascontiguousarray(mesh["cell_nodes"], np.int32)
