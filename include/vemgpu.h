@@ -180,6 +180,15 @@ int vg_solve_host(vg_handle* h, const double* b_host, double* x_host, const vg_s
 int vg_adjoint_grad(vg_handle* h, const double* x, const double* dJdx, double* dJdtheta,
                     const vg_solve_opts* opts, vg_solve_info* info);
 
+/* Assembled sparse matrix of the same operator (a comparator of the matrix-free apply; the
+ * reference's assembled path, MixedGpu::assembled_matrix / coo_matrix / coo_boundary,
+ * vem/CurvedVEM_Darcy_gpu/src/equation_gpu.cu:701-833, which PETSc turns into cuSPARSE CSR).
+ * Reference sign [A, -W^T, L; W, 0, 0; L^T, 0, 0]; constrained = 1 (VG_BC_FLUX) zeroes masked rows
+ * and columns and puts 1 on their diagonal. First call with row_ptr = NULL: *nnz = number of stored
+ * entries (pattern built on the host and kept). Second call: DEVICE arrays row_ptr (N+1, int64,
+ * sorted columns per row), col_idx (nnz) and values (nnz doubles) are filled. */
+int vg_assemble_csr(vg_handle* h, int constrained, long long* nnz, long long* row_ptr, int* col_idx, double* values);
+
 /* ---- post-processing ---------------------------------------------------------------------- */
 
 /* Six figures of MixedGpu::errors (equation_gpu.cu:387-479, 627-648): computational scalar and

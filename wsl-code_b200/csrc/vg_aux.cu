@@ -125,6 +125,87 @@ __global__ void k_contract(const double* A, const int* map, const int* slot_cell
     g[slot_cell[P.slot + lane]] = acc;
 }
 
+// ---- assembled matrix (comparator of the matrix-free apply): CSR values of
+// [A, -W^T, L; W, 0, 0; L^T, 0, 0] in the reference sign, masked rows and columns zeroed and a unit
+// diagonal on masked rows (constrained), every slot receiving at most two addends onto zero
+__device__ __forceinline__ long long csr_find(const long long* rp, const int* ci, long long r, int c) {
+    long long lo = rp[r], hi = rp[r + 1] - 1;
+    while (lo <= hi) {
+        long long mid = (lo + hi) >> 1;
+        int v = ci[mid];
+        if (v == c) return mid;
+        if (v < c)
+            lo = mid + 1;
+        else
+            hi = mid - 1;
+    }
+    return -1;
+}
+
+__global__ void k_assemble(const double* A, const double* W, const int* map, const int* slot_cell, const int* mask,
+                           const double* L, const Piece* pieces, int npieces, int k, long long nf, long long N,
+                           int constrained, int mult, const long long* rp, const int* ci, double* val, int* bad) {
+    Piece P;
+    int lane;
+    if (!slot_of(pieces, npieces, P, lane)) return;
+    const int q = (k + 1) * (k + 2) / 2, n = P.n;
+    const int cell = slot_cell[P.slot + lane];
+    auto add = [&](long long r, long long c, double v) {
+        long long s = csr_find(rp, ci, r, int(c));
+        if (s < 0)
+            atomicExch(bad, 1);
+        else
+            atomicAdd(val + s, v);
+    };
+    auto gdof = [&](int i, double& sg) {
+        int g = map[P.map_off + (long long)i * PIECE + lane];
+        sg = g < 0 ? -1.0 : 1.0;
+        return g < 0 ? ~g : g;
+    };
+    auto masked = [&](long long g) { return constrained && mask[g] != 0; };
+    long long e = 0;
+    for (int i = 0; i < n; ++i) {
+        double si;
+        const long long gi = gdof(i, si);
+        for (int j = i; j < n; ++j, ++e) {
+            double sj;
+            const long long gj = gdof(j, sj);
+            if (masked(gi) || masked(gj)) continue;
+            const double a = A[P.a_off + e * PIECE + lane] * si * sj;
+            add(gi, gj, a);
+            if (j != i) add(gj, gi, a);
+        }
+    }
+    for (int r = 0; r < q; ++r) {
+        const long long pr = nf + (long long)cell * q + r;
+        for (int i = 0; i < n; ++i) {
+            double si;
+            const long long gi = gdof(i, si);
+            if (masked(gi)) continue;
+            const double w = (k == 0 ? 1.0 : W[P.w_off + (long long)(r * n + i) * PIECE + lane]) * si;
+            add(gi, pr, -w);
+            add(pr, gi, w);
+        }
+        if (mult) {
+            const double l = L[(long long)cell * q + r];
+            add(pr, N - 1, l);
+            add(N - 1, pr, l);
+        }
+    }
+}
+
+__global__ void k_assemble_mask(const int* mask, long long N, const long long* rp, const int* ci, double* val,
+                                int* bad) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < N; g += (long long)gridDim.x * blockDim.x)
+        if (mask[g]) {
+            long long s = csr_find(rp, ci, g, int(g));
+            if (s < 0)
+                atomicExch(bad, 1);
+            else
+                val[s] = 1.0;
+        }
+}
+
 __global__ void k_axpy64(double* x, const double* d, double a, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         x[i] += a * d[i];
@@ -175,6 +256,19 @@ void contract_adjoint(const double* A, const int* map, const int* slot_cell, con
     k_contract<<<blocks_for((long long)npieces * PIECE), 256, 0, s>>>(A, map, slot_cell, mask, pieces, npieces, k, x, mu,
                                                                       constrained, g);
     VG_CUDA(cudaGetLastError());
+}
+
+void assemble_values(const double* A, const double* W, const int* map, const int* slot_cell, const int* mask,
+                     const double* L, const Piece* pieces, int npieces, int k, long long nf, long long N,
+                     int constrained, int mult, const long long* rp, const int* ci, double* val, int* bad,
+                     cudaStream_t s) {
+    k_assemble<<<blocks_for((long long)npieces * PIECE), 256, 0, s>>>(A, W, map, slot_cell, mask, L, pieces, npieces, k,
+                                                                       nf, N, constrained, mult, rp, ci, val, bad);
+    VG_CUDA(cudaGetLastError());
+    if (constrained) {
+        k_assemble_mask<<<148 * 4, 256, 0, s>>>(mask, N, rp, ci, val, bad);
+        VG_CUDA(cudaGetLastError());
+    }
 }
 
 void axpy64_kernel_launch(double* x, const double* d, double a, long long n, cudaStream_t s) {

@@ -226,6 +226,13 @@ int vg_errors_noalloc(vg_handle* h, const double* x, double out[6]) {
     });
 }
 
+int vg_assemble_csr(vg_handle* h, int constrained, long long* nnz, long long* row_ptr, int* col_idx, double* values) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!nnz) throw vg::Error(VG_EINVAL, "null nnz");
+        s.assemble(constrained, nnz, row_ptr, col_idx, values);
+    });
+}
+
 int vg_local(vg_handle* h, int cell, int which, double* out, int* count) {
     return guarded(h, [&](vg::Solver& s) {
         int c = s.local(cell, which, out);

@@ -21,6 +21,10 @@ void diag_invert(double* d, const int* mask, const double* contrib, int nc, long
 void lift_rhs(const int* mask, const double* g, const double* y, double* b, long long N, cudaStream_t s);
 void rescale_ops(const double* theta, const int* slot_cell, const Piece* pieces, int npieces, const double* A0,
                  double* A64, float* A32, cudaStream_t s);
+void assemble_values(const double* A, const double* W, const int* map, const int* slot_cell, const int* mask,
+                     const double* L, const Piece* pieces, int npieces, int k, long long nf, long long N,
+                     int constrained, int mult, const long long* rp, const int* ci, double* val, int* bad,
+                     cudaStream_t s);
 void contract_adjoint(const double* A, const int* map, const int* slot_cell, const int* mask, const Piece* pieces,
                       int npieces, int k, const double* x, const double* mu, int constrained, double* g,
                       cudaStream_t s);
@@ -983,6 +987,90 @@ void Solver::solve_host(const double* b_host, double* x_host, const vg_solve_opt
     solve(d_hb_.data(), d_hx_.data(), o, info, nullptr);
     VG_CUDA(cudaMemcpyAsync(x_host, d_hx_.data(), sizeof(double) * N, cudaMemcpyDeviceToHost, stream_));
     VG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+// sparsity pattern of the assembled system (host, cached): row g of a flux dof holds the dofs of
+// the cells around g, a pressure row the dofs of its cell, the multiplier row every pressure dof;
+// every row holds its diagonal (the unit diagonal of masked rows)
+void Solver::assembled_pattern() {
+    if (!csr_ptr_.empty()) return;
+    const bool mult = bc == VG_BC_FLUX;
+    auto dofs_of = [&](int c, std::vector<int>& out) {
+        const int slot = cell_slot_[c];
+        const Piece& P = pieces_[slot / PIECE];
+        const int lane = slot % PIECE;
+        for (int i = 0; i < P.n; ++i) {
+            int g = map_host_[P.map_off + (long long)i * PIECE + lane];
+            out.push_back(g < 0 ? ~g : g);
+        }
+        for (int r = 0; r < q; ++r) out.push_back(nf + c * q + r);
+        if (mult) out.push_back(N - 1);
+    };
+    // cells around every flux dof
+    std::vector<int> cnt(nf + 1, 0), cells;
+    std::vector<int> tmp;
+    for (int c = 0; c < m.nc; ++c) {
+        tmp.clear();
+        dofs_of(c, tmp);
+        for (int g : tmp)
+            if (g < nf) cnt[g + 1]++;
+    }
+    for (int g = 0; g < nf; ++g) cnt[g + 1] += cnt[g];
+    cells.assign(cnt[nf], 0);
+    {
+        std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+        for (int c = 0; c < m.nc; ++c) {
+            tmp.clear();
+            dofs_of(c, tmp);
+            for (int g : tmp)
+                if (g < nf) cells[fill[g]++] = c;
+        }
+    }
+    csr_ptr_.assign(size_t(N) + 1, 0);
+    csr_col_.clear();
+    std::vector<int> row;
+    auto emit = [&](long long r) {
+        row.push_back(int(r));
+        std::sort(row.begin(), row.end());
+        row.erase(std::unique(row.begin(), row.end()), row.end());
+        csr_col_.insert(csr_col_.end(), row.begin(), row.end());
+        csr_ptr_[r + 1] = (long long)csr_col_.size();
+    };
+    for (int g = 0; g < nf; ++g) {
+        row.clear();
+        for (int t = cnt[g]; t < cnt[g + 1]; ++t) dofs_of(cells[t], row);
+        emit(g);
+    }
+    for (int c = 0; c < m.nc; ++c)
+        for (int r = 0; r < q; ++r) {
+            row.clear();
+            dofs_of(c, row);
+            emit(nf + (long long)c * q + r);
+        }
+    if (mult) {
+        row.clear();
+        for (long long i = nf; i < nf + np; ++i) row.push_back(int(i));
+        emit(N - 1);
+    }
+}
+
+void Solver::assemble(int constrained, long long* nnz, long long* rp, int* ci, double* val) {
+    if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_assemble_csr");
+    assembled_pattern();
+    *nnz = (long long)csr_col_.size();
+    if (!rp) return;
+    if (!ci || !val) throw Error(VG_EINVAL, "vg_assemble_csr needs row_ptr, col_idx and values");
+    VG_CUDA(cudaMemcpy(rp, csr_ptr_.data(), sizeof(long long) * csr_ptr_.size(), cudaMemcpyHostToDevice));
+    VG_CUDA(cudaMemcpy(ci, csr_col_.data(), sizeof(int) * csr_col_.size(), cudaMemcpyHostToDevice));
+    VG_CUDA(cudaMemset(val, 0, sizeof(double) * csr_col_.size()));
+    DevBuf<int> bad(1);
+    bad.zero();
+    assemble_values(d_A64_.data(), d_W64_.data(), d_map_.data(), d_slot_cell_.data(), d_mask_.data(), d_L_.data(),
+                    d_pieces_.data(), int(pieces_.size()), k, nf, N, (constrained && bc == VG_BC_FLUX) ? 1 : 0,
+                    bc == VG_BC_FLUX ? 1 : 0, rp, ci, val, bad.data(), nullptr);
+    int b = 0;
+    VG_CUDA(cudaMemcpy(&b, bad.data(), sizeof(int), cudaMemcpyDeviceToHost));
+    if (b) throw Error(VG_ESTATE, "assembled pattern does not hold an entry of a local block");
 }
 
 void Solver::axpy64(double* x, const double* d, double a, cudaStream_t s) {

@@ -60,6 +60,8 @@ public:
     // same figures with the per-cell scratch in a static device array (no device allocation)
     void errors_static(const double* x, double out[6]);
     int local(int cell, int which, double* out);
+    // assembled CSR of the system (comparator of the matrix-free apply); rp == nullptr: size only
+    void assemble(int constrained, long long* nnz, long long* rp, int* ci, double* val);
 
     // sizes
     int k, nq, ng, q, p, ngrad, internal, nf, np, N, maxn;
@@ -84,6 +86,9 @@ private:
     void lift_flux_rhs();
     void build_amg();
     void build_amg_high();
+    void assembled_pattern();
+    std::vector<long long> csr_ptr_;  // assembled pattern (host, built on first request)
+    std::vector<int> csr_col_;
     void check_status(const char* where);
     void axpy64(double* x, const double* d, double a, cudaStream_t s);
     void minres(bool fp32, const void* b, void* x, double tol, int maxit, int check_every, int& iters,

@@ -77,6 +77,7 @@ def lib():
         L.vg_errors.argtypes = [P, P, P]
         L.vg_errors_noalloc.argtypes = [P, P, P]
         L.vg_local.argtypes = [P, I, I, P, ctypes.POINTER(I)]
+        L.vg_assemble_csr.argtypes = [P, I, ctypes.POINTER(LL), P, P, P]
         L.vg_stats.argtypes = [P, P]
         _lib = L
     return _lib

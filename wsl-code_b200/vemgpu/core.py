@@ -188,6 +188,19 @@ class DarcyGpu:
         L.check(L.lib().vg_errors(self.h, x.data_ptr(), out), self.h)
         return dict(zip(("scalar_comp", "flux_comp", "scalar_phys", "flux_phys", "div_phys", "mass"), list(out)))
 
+    def assemble_csr(self, constrained=True):
+        """Assembled system as a torch sparse CSR tensor on the device (vg_assemble_csr; reference
+        sign). A comparator of the matrix-free apply: its SpMV runs in cuSPARSE."""
+        torch = _torch()
+        nnz = ctypes.c_longlong(0)
+        L.check(L.lib().vg_assemble_csr(self.h, int(constrained), ctypes.byref(nnz), None, None, None), self.h)
+        rp = torch.empty(self.N + 1, dtype=torch.int64, device="cuda")
+        ci = torch.empty(nnz.value, dtype=torch.int32, device="cuda")
+        val = torch.empty(nnz.value, dtype=torch.float64, device="cuda")
+        L.check(L.lib().vg_assemble_csr(self.h, int(constrained), ctypes.byref(nnz), rp.data_ptr(), ci.data_ptr(),
+                                        val.data_ptr()), self.h)
+        return torch.sparse_csr_tensor(rp, ci.long(), val, size=(self.N, self.N))
+
     def stats(self):
         out = (ctypes.c_longlong * 4)()
         L.check(L.lib().vg_stats(self.h, out), self.h)
