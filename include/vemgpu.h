@@ -189,6 +189,25 @@ int vg_adjoint_grad(vg_handle* h, const double* x, const double* dJdx, double* d
  * sorted columns per row), col_idx (nnz) and values (nnz doubles) are filled. */
 int vg_assemble_csr(vg_handle* h, int constrained, long long* nnz, long long* row_ptr, int* col_idx, double* values);
 
+/* Physical cell measures int_E det J (device, num_cells doubles); the reference keeps them in
+ * Cell::area of its device records (vem/CurvedVEM_Darcy_gpu/include/device.cuh:107-134). */
+int vg_cell_areas(vg_handle* h, double* areas);
+
+/* ---- ternary Maxwell-Stefan diffusion (k = 0) ------------------------------------------------
+ * Replaces the reference's Maxwell-Stefan driver (MSGpu, vem/CurvedVEM_Darcy_gpu/include/equation_gpu.cuh:122-127,
+ * run_case time loop src/solver_driver.cpp:189-245), in the reduced two-species form with
+ * diffusivities D12, D13, D23: backward Euler, one coupled saddle-point system per step with the
+ * friction matrix frozen at x^n, no flux through the boundary (the handle must be built with
+ * VG_BC_FLUX; its K = I operator is used whatever the permeability). State vector (device doubles):
+ * [J1 (nf), J2 (nf), x1 (num_cells), x2 (num_cells)], x3 = 1 - x1 - x2. */
+int vg_ms_configure(vg_handle* h, double d12, double d13, double d23, double dt, long long* state_size);
+/* y = K(coeff_state) x for the Maxwell-Stefan system (FP64 or FP32 x, y; device). */
+int vg_ms_apply(vg_handle* h, const double* coeff_state, const void* x, void* y, int precision);
+/* One backward-Euler step: solve K(old) new = [0; |E|/dt x_old] to ||b - K new|| / ||b|| <= opts->tol
+ * by right-preconditioned GMRES(30), FP64 or FP32 inner under FP64 refinement (opts->mode). */
+int vg_ms_step(vg_handle* h, const double* old_state, double* new_state, const vg_solve_opts* opts,
+               vg_solve_info* info);
+
 /* ---- post-processing ---------------------------------------------------------------------- */
 
 /* Six figures of MixedGpu::errors (equation_gpu.cu:387-479, 627-648): computational scalar and

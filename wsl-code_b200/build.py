@@ -21,7 +21,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "vemgpu")
 OBJ = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(ROOT, "include")
-CUDA_UNITS = ["vg_mesh", "vg_setup", "vg_apply", "vg_krylov", "vg_aux", "vg_amg", "vg_solver", "vg_capi"]
+CUDA_UNITS = ["vg_mesh", "vg_setup", "vg_apply", "vg_krylov", "vg_aux", "vg_amg", "vg_solver", "vg_ms", "vg_capi"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 LIB = os.path.join(OUT, "libvemgpu.so")

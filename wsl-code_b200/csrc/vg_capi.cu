@@ -233,6 +233,47 @@ int vg_assemble_csr(vg_handle* h, int constrained, long long* nnz, long long* ro
     });
 }
 
+int vg_cell_areas(vg_handle* h, double* areas) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!areas) throw vg::Error(VG_EINVAL, "null vector");
+        s.cell_areas(areas);
+    });
+}
+
+int vg_ms_configure(vg_handle* h, double d12, double d13, double d23, double dt, long long* state_size) {
+    return guarded(h, [&](vg::Solver& s) {
+        s.ms_configure(d12, d13, d23, dt);
+        if (state_size) *state_size = s.ms_size();
+    });
+}
+
+int vg_ms_apply(vg_handle* h, const double* coeff_state, const void* x, void* y, int precision) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!coeff_state || !x || !y || x == y) throw vg::Error(VG_EINVAL, "null or aliased vector");
+        s.ms_coefficients(coeff_state);
+        if (precision == VG_FP64)
+            s.ms_apply(static_cast<const double*>(x), static_cast<double*>(y));
+        else if (precision == VG_FP32)
+            s.ms_apply(static_cast<const float*>(x), static_cast<float*>(y));
+        else
+            throw vg::Error(VG_EINVAL, "precision must be VG_FP64 or VG_FP32");
+        VG_CUDA(cudaDeviceSynchronize());
+    });
+}
+
+int vg_ms_step(vg_handle* h, const double* old_state, double* new_state, const vg_solve_opts* opts,
+               vg_solve_info* info) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!old_state || !new_state) throw vg::Error(VG_EINVAL, "null state");
+        vg_solve_opts o;
+        vg_default_solve_opts(&o);
+        if (opts) o = *opts;
+        vg_solve_info inf{};
+        s.ms_step(old_state, new_state, o, inf);
+        if (info) *info = inf;
+    });
+}
+
 int vg_local(vg_handle* h, int cell, int which, double* out, int* count) {
     return guarded(h, [&](vg::Solver& s) {
         int c = s.local(cell, which, out);

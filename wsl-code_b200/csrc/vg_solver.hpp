@@ -60,6 +60,14 @@ public:
     // same figures with the per-cell scratch in a static device array (no device allocation)
     void errors_static(const double* x, double out[6]);
     int local(int cell, int which, double* out);
+    // Maxwell-Stefan (k = 0, no-flux boundary): state [J1 (nf), J2 (nf), x1 (nc), x2 (nc)]
+    void ms_configure(double d12, double d13, double d23, double dt);
+    void ms_step(const double* old_state, double* new_state, const vg_solve_opts& o, vg_solve_info& info);
+    void ms_coefficients(const double* state);
+    template <typename T>
+    void ms_apply(const T* x, T* y);
+    long long ms_size() const { return ms_.N; }
+    void cell_areas(double* out);
     // assembled CSR of the system (comparator of the matrix-free apply); rp == nullptr: size only
     void assemble(int constrained, long long* nnz, long long* rp, int* ci, double* val);
 
@@ -86,6 +94,19 @@ private:
     void lift_flux_rhs();
     void build_amg();
     void build_amg_high();
+    template <typename T>
+    void ms_precond(const T* r, T* z);
+    template <typename T>
+    void ms_dots(const T* V, long long ld, int cnt, const T* w, double* out);
+    template <typename T>
+    int ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* rel);
+    struct MsState {
+        bool ready = false;
+        double i12 = 0, i13 = 0, i23 = 0, dt = 0;
+        long long N = 0;
+        DevBuf<double> B64, F64, C64, D, m64, V64, b, r, y, d, t64, w64, partials, h;
+        DevBuf<float> B32, F32, C32, m32, A32, V32, r32, d32, t32, w32;
+    } ms_;
     void assembled_pattern();
     std::vector<long long> csr_ptr_;  // assembled pattern (host, built on first request)
     std::vector<int> csr_col_;

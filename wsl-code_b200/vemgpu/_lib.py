@@ -78,6 +78,10 @@ def lib():
         L.vg_errors_noalloc.argtypes = [P, P, P]
         L.vg_local.argtypes = [P, I, I, P, ctypes.POINTER(I)]
         L.vg_assemble_csr.argtypes = [P, I, ctypes.POINTER(LL), P, P, P]
+        L.vg_cell_areas.argtypes = [P, P]
+        L.vg_ms_configure.argtypes = [P, D, D, D, D, ctypes.POINTER(LL)]
+        L.vg_ms_apply.argtypes = [P, P, P, P, I]
+        L.vg_ms_step.argtypes = [P, P, P, ctypes.POINTER(VgSolveOpts), ctypes.POINTER(VgSolveInfo)]
         L.vg_stats.argtypes = [P, P]
         _lib = L
     return _lib
