@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-assembled", action="store_true", help="skip the assembled cuSPARSE comparator")
     ap.add_argument("--no-config1", action="store_true", help="skip the 250k-cell disk k=0/k=1 leg")
     ap.add_argument("--config1-cells", type=int, default=250000)
+    ap.add_argument("--no-ms", action="store_true", help="skip the Maxwell-Stefan leg")
+    ap.add_argument("--ms-steps", type=int, default=100)
     ap.add_argument("--eager", action="store_true", help="with --profile: host-driven Krylov batches, no graph")
     return ap.parse_args()
 
@@ -276,6 +278,44 @@ def assembled_leg(g, z32, z64, stream_ms):
     return out
 
 
+def ms_leg(args):
+    """Ternary Maxwell-Stefan on the 250k-cell disk: D12 = 1, D13 = 0.5, D23 = 0.2, seeded smooth
+    initial fractions in [0.1, 0.8] summing to 1, backward Euler dt = 1e-3, 100 steps; FP64 and
+    FP32-refined runs (each step to 1e-10), sum-to-one, bounds and species masses checked every step."""
+    import numpy as np
+    import torch
+    from vemgpu.maxwell_stefan import MaxwellStefan, initial_fractions
+    mesh = disk_mesh(args.config1_cells, args.seed)
+    ms = MaxwellStefan(mesh, D=(1.0, 0.5, 0.2), dt=1e-3)
+    x1, x2, _ = initial_fractions(mesh, seed=args.seed + 31)
+    s0 = ms.state(x1, x2)
+    m0 = ms.masses(s0)
+    out = {"cells": ms.nc, "unknowns": ms.N, "steps": args.ms_steps, "dt": 1e-3, "D": [1.0, 0.5, 0.2]}
+    finals = {}
+    for mode in ("fp64", "mixed"):
+        s = s0.clone()
+        its, secs, sum_err, mass_err, lo, hi = [], [], 0.0, 0.0, 1.0, 0.0
+        for _ in range(args.ms_steps):
+            s, info = ms.step(s, mode=mode, tol=1e-10, inner_tol=1e-5)
+            its.append(info["iterations"])
+            secs.append(info["seconds"])
+            f = ms.fractions(s)
+            sum_err = max(sum_err, float(torch.abs(f[0] + f[1] + f[2] - 1).max()))
+            lo = min(lo, min(float(x.min()) for x in f))
+            hi = max(hi, max(float(x.max()) for x in f))
+            mass_err = max(mass_err, max(abs(a - b) / abs(b) for a, b in zip(ms.masses(s), m0)))
+        finals[mode] = torch.cat(ms.fractions(s)[:2])
+        out[mode] = {"total_s": float(np.sum(secs)), "step_ms_mean": 1e3 * float(np.mean(secs)),
+                     "iterations_mean": float(np.mean(its)), "iterations_max": int(np.max(its)),
+                     "max_sum_to_one_error": sum_err, "max_rel_mass_change": mass_err, "min_fraction": lo,
+                     "max_fraction": hi}
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["total_s"] / out["mixed"]["total_s"]
+    out["final_rel_diff_mixed_vs_fp64"] = float(torch.linalg.norm(finals["mixed"] - finals["fp64"]) /
+                                                torch.linalg.norm(finals["fp64"]))
+    ms.close()
+    return out
+
+
 def config1_leg(args):
     """Disk problem of the reference's own examples at 250k cells: p = sin(pi x) sin(pi y), Dirichlet
     pressure, K = I, k = 0 and k = 1, FP64 and mixed solves to 1e-10 (device time) and the L2 errors
@@ -445,6 +485,7 @@ def ours(args, rank, world, dist):
     e2e_s = max_over_ranks(sum(e2e) / len(e2e), dist)
     adjoint = None if args.no_adjoint else adjoint_leg(args, rank)
     config1 = None if args.no_config1 else config1_leg(args)
+    ms = None if args.no_ms else ms_leg(args)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
         threads = 1
@@ -482,6 +523,7 @@ def ours(args, rank, world, dist):
         "assembled_comparator": assembled,
         "adjoint": adjoint,
         "disk_250k": config1,
+        "maxwell_stefan": ms,
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,

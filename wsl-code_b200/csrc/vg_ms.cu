@@ -14,9 +14,10 @@
 // B is not symmetric, so the system is solved by right-preconditioned GMRES(m) (classical
 // Gram-Schmidt applied twice, device vectors, Hessenberg and Givens rotations on the host), FP64 or
 // FP32 inner under FP64 iterative refinement, with a block-diagonal preconditioner: the 2x2 species
-// block of the assembled flux diagonal per flux dof, and per cell the 2x2 block
-// (|E|/dt) I + sum_i F_{g_i}^{-1} (diagonal of the Schur complement). The time-step mass term keeps
-// the Schur complement well conditioned at the configured dt, so no multigrid is needed here.
+// block of the assembled flux diagonal per flux dof, and for each species one smoothed-aggregation
+// V-cycle on its pressure Schur block (|E|/dt) I + W diag(F^{-1})_ss W^T (without the hierarchy:
+// the 2x2 cell blocks (|E|/dt) I + sum_i F_{g_i}^{-1}). The hierarchy is built from the first state
+// stepped after configuration and kept (a fixed preconditioner for GMRES).
 #include <algorithm>
 #include <cmath>
 
@@ -211,18 +212,22 @@ __global__ void k_ms_pc_apply(const T* r, T* z, const T* F, const T* C, long lon
 
 // partial dot products of w with the first cnt columns of V (column stride ld), one row of
 // MS_MAXM partials per block
+// (with self: w.w in slot cnt, cnt < MS_MAXM)
 template <typename T>
 __global__ void __launch_bounds__(MS_THREADS) k_mdot(const T* V, long long ld, int cnt, const T* w, long long n,
-                                                     double* partials) {
+                                                     double* partials, int self) {
     double acc[MS_MAXM];
 #pragma unroll
     for (int k = 0; k < MS_MAXM; ++k) acc[k] = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double wi = double(w[i]);
 #pragma unroll
-        for (int k = 0; k < MS_MAXM; ++k)
+        for (int k = 0; k < MS_MAXM; ++k) {
             if (k < cnt) acc[k] += double(V[k * ld + i]) * wi;
+            if (self && k == cnt) acc[k] += wi * wi;
+        }
     }
+    cnt += self;
     __shared__ double sh[MS_THREADS / 32][MS_MAXM];
     const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
 #pragma unroll
@@ -349,6 +354,7 @@ void Solver::ms_configure(double d12, double d13, double d23, double dt) {
     ms_.partials.resize(size_t(MS_BLOCKS) * MS_MAXM);
     ms_.h.resize(MS_MAXM);
     VG_CUDA(cudaDeviceSynchronize());
+    ms_.amg_ready = false;
     ms_.ready = true;
 }
 
@@ -386,15 +392,66 @@ void Solver::ms_precond(const T* r, T* z) {
     const T* C = sizeof(T) == 8 ? reinterpret_cast<const T*>(ms_.C64.data()) : reinterpret_cast<const T*>(ms_.C32.data());
     k_ms_pc_apply<T><<<MS_BLOCKS, MS_THREADS>>>(r, z, F, C, nf, m.nc);
     VG_CUDA(cudaGetLastError());
+    if (ms_.amg_ready)  // pressure blocks: one V-cycle per species (replaces the 2x2 cell blocks)
+        for (int s = 0; s < 2; ++s)
+            ms_.amg[s].vcycle(r + 2 * nf + (long long)s * m.nc, z + 2 * nf + (long long)s * m.nc, nullptr);
+}
+
+// S_s = diag(|E|/dt) + W diag((F_g^{-1})_ss) W^T on the cell graph (k = 0: W = +-1 per local edge,
+// opposite signs across a shared edge), free flux dofs only
+void Solver::ms_build_amg() {
+    std::vector<double> F = ms_.F64.download(), mdt = ms_.m64.download();
+    std::vector<int> mask(nf);
+    VG_CUDA(cudaMemcpy(mask.data(), d_mask_.data(), sizeof(int) * nf, cudaMemcpyDeviceToHost));
+    std::vector<int> ec(2 * size_t(m.ne), -1);
+    for (int c = 0; c < m.nc; ++c)
+        for (int j = m.cptr[c]; j < m.cptr[c + 1]; ++j) {
+            int e = m.gedges[j];
+            if (ec[2 * e] < 0)
+                ec[2 * e] = c;
+            else
+                ec[2 * e + 1] = c;
+        }
+    for (int s = 0; s < 2; ++s) {
+        HostCsr S;
+        S.n = S.m = m.nc;
+        S.ptr.assign(m.nc + 1, 0);
+        std::vector<std::pair<int, double>> row;
+        for (int c = 0; c < m.nc; ++c) {
+            row.clear();
+            double diag = mdt[c];
+            for (int j = m.cptr[c]; j < m.cptr[c + 1]; ++j) {
+                int e = m.gedges[j];
+                if (mask[e]) continue;
+                const double w = F[4 * size_t(e) + 3 * s];
+                diag += w;
+                int o = ec[2 * e] == c ? ec[2 * e + 1] : ec[2 * e];
+                if (o >= 0) row.push_back({o, -w});
+            }
+            row.push_back({c, diag});
+            std::sort(row.begin(), row.end());
+            for (size_t i = 0; i < row.size(); ++i) {
+                if (i > 0 && row[i].first == row[i - 1].first) {
+                    S.val.back() += row[i].second;
+                    continue;
+                }
+                S.col.push_back(row[i].first);
+                S.val.push_back(row[i].second);
+            }
+            S.ptr[c + 1] = int(S.col.size());
+        }
+        ms_.amg[s].setup(S, nullptr);
+    }
+    ms_.amg_ready = true;
 }
 
 // dot products of w with columns 0..cnt-1 of V (host result)
 template <typename T>
-void Solver::ms_dots(const T* V, long long ld, int cnt, const T* w, double* out) {
-    k_mdot<T><<<MS_BLOCKS, MS_THREADS>>>(V, ld, cnt, w, ms_.N, ms_.partials.data());
-    k_mdot_finish<<<1, MS_MAXM>>>(ms_.partials.data(), MS_BLOCKS, cnt, ms_.h.data());
+void Solver::ms_dots(const T* V, long long ld, int cnt, const T* w, double* out, int self) {
+    k_mdot<T><<<MS_BLOCKS, MS_THREADS>>>(V, ld, cnt, w, ms_.N, ms_.partials.data(), self);
+    k_mdot_finish<<<1, MS_MAXM>>>(ms_.partials.data(), MS_BLOCKS, cnt + self, ms_.h.data());
     VG_CUDA(cudaGetLastError());
-    VG_CUDA(cudaMemcpy(out, ms_.h.data(), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+    VG_CUDA(cudaMemcpy(out, ms_.h.data(), sizeof(double) * (cnt + self), cudaMemcpyDeviceToHost));
 }
 
 // right-preconditioned GMRES(m) on K d = r from d = 0; returns iterations, relative reduction in *rel
@@ -409,13 +466,13 @@ int Solver::ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* 
     // residual of the current iterate, kept in t (r initially)
     VG_CUDA(cudaMemcpyAsync(t, r, sizeof(T) * Nm, cudaMemcpyDeviceToDevice, nullptr));
     double nr = 0;
-    ms_dots(t, 0, 1, t, &nr);
+    ms_dots(t, 0, 1, t, &nr, 0);
     const double beta0 = std::sqrt(nr);
     *rel = 1.0;
     if (!(beta0 > 0)) return 0;
     int its = 0;
-    std::vector<double> H(size_t(MS_MAXM) * MS_MAXM), cs(MS_MAXM), sn(MS_MAXM), g(MS_MAXM + 1), h(MS_MAXM), h2(MS_MAXM),
-        y(MS_MAXM);
+    std::vector<double> H(size_t(MS_MAXM) * MS_MAXM), cs(MS_MAXM), sn(MS_MAXM), g(MS_MAXM + 1), h(MS_MAXM + 1),
+        h2(MS_MAXM), y(MS_MAXM);
     double beta = beta0;
     while (its < maxit) {
         k_scale_to<T><<<MS_BLOCKS, MS_THREADS>>>(t, 1.0 / beta, V, Nm);
@@ -427,15 +484,17 @@ int Solver::ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* 
             ++its;
             ms_precond<T>(V + (long long)j * Nm, t);
             ms_apply<T>(t, w);
-            ms_dots(V, Nm, j + 1, w, h.data());
+            // classical Gram-Schmidt applied twice (the second pass restores orthogonality lost to
+            // cancellation); the norm of the result rides on the second projection's pass
+            ms_dots(V, Nm, j + 1, w, h.data(), 0);
             VG_CUDA(cudaMemcpy(ms_.h.data(), h.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice));
             k_gs_update<T><<<MS_BLOCKS, MS_THREADS>>>(V, Nm, j + 1, ms_.h.data(), w, Nm);
-            ms_dots(V, Nm, j + 1, w, h2.data());
+            ms_dots(V, Nm, j + 1, w, h2.data(), 0);
             VG_CUDA(cudaMemcpy(ms_.h.data(), h2.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice));
             k_gs_update<T><<<MS_BLOCKS, MS_THREADS>>>(V, Nm, j + 1, ms_.h.data(), w, Nm);
             for (int i = 0; i <= j; ++i) h[i] += h2[i];
             double nw = 0;
-            ms_dots(w, 0, 1, w, &nw);
+            ms_dots(w, 0, 1, w, &nw, 0);
             const double hn = std::sqrt(std::max(nw, 0.0));
             if (hn > 0) k_scale_to<T><<<MS_BLOCKS, MS_THREADS>>>(w, 1.0 / hn, V + (long long)(j + 1) * Nm, Nm);
             // Givens rotations of column j
@@ -480,7 +539,7 @@ int Solver::ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* 
             k_axpy_t<T><<<MS_BLOCKS, MS_THREADS>>>(t, w, -1.0, Nm);
         }
         double nt = 0;
-        ms_dots(t, 0, 1, t, &nt);
+        ms_dots(t, 0, 1, t, &nt, 0);
         beta = std::sqrt(nt);
         *rel = beta / beta0;
         if (*rel <= tol || !(beta > 0)) break;
@@ -525,6 +584,14 @@ void Solver::ms_step(const double* old_state, double* new_state, const vg_solve_
     k_ms_pc_cell<<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS>>>(
         d_map_.data(), d_pieces_.data(), int(pieces_.size()), d_slot_cell_.data(), d_mask_.data(), ms_.F64.data(),
         ms_.m64.data(), ms_.C64.data(), ms_.C32.data());
+    if (!ms_.amg_ready) {
+        VG_CUDA(cudaDeviceSynchronize());
+        try {
+            ms_build_amg();
+        } catch (const Error&) {
+            ms_.amg_ready = false;  // the 2x2 cell blocks stay in use
+        }
+    }
     k_ms_rhs<<<MS_BLOCKS, MS_THREADS>>>(old_state, ms_.m64.data(), nf, m.nc, ms_.b.data());
     VG_CUDA(cudaGetLastError());
     // initial guess: the old state
@@ -534,8 +601,8 @@ void Solver::ms_step(const double* old_state, double* new_state, const vg_solve_
         ms_apply<double>(new_state, ms_.y.data());
         k_sub<<<MS_BLOCKS, MS_THREADS>>>(ms_.b.data(), ms_.y.data(), ms_.r.data(), Nm);
         double nr = 0, nb = 0;
-        ms_dots(ms_.r.data(), 0, 1, ms_.r.data(), &nr);
-        ms_dots(ms_.b.data(), 0, 1, ms_.b.data(), &nb);
+        ms_dots(ms_.r.data(), 0, 1, ms_.r.data(), &nr, 0);
+        ms_dots(ms_.b.data(), 0, 1, ms_.b.data(), &nb, 0);
         if (nb_out) *nb_out = std::sqrt(nb);
         return std::sqrt(nr) / (nb > 0 ? std::sqrt(nb) : 1.0);
     };

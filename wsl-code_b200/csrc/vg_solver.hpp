@@ -97,7 +97,7 @@ private:
     template <typename T>
     void ms_precond(const T* r, T* z);
     template <typename T>
-    void ms_dots(const T* V, long long ld, int cnt, const T* w, double* out);
+    void ms_dots(const T* V, long long ld, int cnt, const T* w, double* out, int self);
     template <typename T>
     int ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* rel);
     struct MsState {
@@ -106,7 +106,12 @@ private:
         long long N = 0;
         DevBuf<double> B64, F64, C64, D, m64, V64, b, r, y, d, t64, w64, partials, h;
         DevBuf<float> B32, F32, C32, m32, A32, V32, r32, d32, t32, w32;
+        // per-species multigrid of the pressure Schur block, built from the first state stepped
+        // after vg_ms_configure and kept for the following steps
+        Amg amg[2];
+        bool amg_ready = false;
     } ms_;
+    void ms_build_amg();
     void assembled_pattern();
     std::vector<long long> csr_ptr_;  // assembled pattern (host, built on first request)
     std::vector<int> csr_col_;
