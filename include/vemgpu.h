@@ -154,6 +154,15 @@ int vg_build(vg_handle* h);
  * Replaces MixedGpu::apply (vem/CurvedVEM_Darcy_gpu/src/equation_gpu.cu:580-598). */
 int vg_apply(vg_handle* h, const void* x, void* y, int precision, int constrained, void* stream);
 
+/* Internally the solver numbers the flux unknowns by first use in its cell layout and the pressure
+ * rows by cell layout, so that the apply's gathers and scatters coalesce; vg_apply and vg_solve
+ * permute at the boundary. A caller that runs many applies (its own Krylov loop) can keep vectors
+ * in that order: vg_permute(h, 1, x, xi, ...) maps the reference order to the internal one
+ * (0: back), and vg_apply with precision | VG_ORDER_INTERNAL takes and returns internal-order
+ * vectors (no permutation). No counterpart in the reference. */
+#define VG_ORDER_INTERNAL 0x100
+int vg_permute(vg_handle* h, int to_internal, const void* in, void* out, int precision, void* stream);
+
 /* Right-hand side of the constrained system (reference sign, device pointer, N doubles):
  * pressure rows int f m det J, Dirichlet loads on flux rows (VG_BC_PRESSURE) or the lifted rows
  * of MixedGpu::make_rhs (VG_BC_FLUX). */

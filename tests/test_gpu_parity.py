@@ -293,3 +293,16 @@ def test_assembled_csr_arcs_pressure_bc(disk200):
     C = g.assemble_csr()
     K, _ = o.system()
     _close(C.to_dense().cpu().numpy(), K.toarray(), 1e-12)
+
+
+def test_internal_order_apply_and_permute(disk200):
+    """vg_permute and vg_apply with VG_ORDER_INTERNAL: the solver's internal numbering gives the
+    same operator (bitwise, after the permutations)."""
+    _, g = pair(disk200, 1, 9, O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
+    x = torch.randn(g.N, dtype=torch.float64, device="cuda")
+    xi = g.permute(x)
+    assert not torch.equal(xi, x)
+    assert torch.equal(g.permute(xi, to_internal=False), x)
+    y = g.apply(x)
+    yi = g.apply(xi, internal_order=True)
+    assert torch.equal(g.permute(yi, to_internal=False), y)

@@ -74,6 +74,29 @@ HostCsr spgemm(const HostCsr& A, const HostCsr& B) {
     return C;
 }
 
+// rows i -> rows[i] and columns j -> cols[j] (either may be null), columns sorted per row
+HostCsr permute_csr(const HostCsr& S, const std::vector<int>* rows, const std::vector<int>* cols) {
+    HostCsr T;
+    T.n = S.n;
+    T.m = S.m;
+    T.ptr.assign(S.n + 1, 0);
+    std::vector<int> old_of(S.n);
+    for (int i = 0; i < S.n; ++i) old_of[rows ? (*rows)[i] : i] = i;
+    std::vector<std::pair<int, double>> row;
+    for (int t = 0; t < S.n; ++t) {
+        const int i = old_of[t];
+        row.clear();
+        for (int j = S.ptr[i]; j < S.ptr[i + 1]; ++j) row.push_back({cols ? (*cols)[S.col[j]] : S.col[j], S.val[j]});
+        std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (const auto& e : row) {
+            T.col.push_back(e.first);
+            T.val.push_back(e.second);
+        }
+        T.ptr[t + 1] = int(T.col.size());
+    }
+    return T;
+}
+
 double diag_of(const HostCsr& A, int i) {
     for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j)
         if (A.col[j] == i) return A.val[j];
@@ -443,7 +466,7 @@ long long Amg::nnz() const {
     return t;
 }
 
-void Amg::setup(const HostCsr& S0, const HostCsr* first_P) {
+void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int>* fine_order) {
     PhaseTimer pt;
     levels_.clear();
     HostCsr A = S0;
@@ -501,8 +524,18 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P) {
                     }
                 }
         };
-        to_sell(A, L.A, levels_.empty());
+        // the finest level is coarsened in the given matrix's order (aggregation visits rows in
+        // order) and stored in fine_order, the order of the vectors it will act on
+        const bool fine = levels_.empty() && fine_order;
+        const std::vector<double> dinv_own(L.dinv);  // in A's own order (smoothing, spectral radius)
+        if (fine) {
+            for (int i = 0; i < A.n; ++i) L.dinv[(*fine_order)[i]] = dinv_own[i];
+            to_sell(permute_csr(A, fine_order, fine_order), L.A, true);
+        } else {
+            to_sell(A, L.A, levels_.empty());
+        }
         if (A.n <= COARSE_MAX || levels_.size() >= 16) {
+            if (fine) A = permute_csr(A, fine_order, fine_order);
             levels_.push_back(std::move(L));
             break;
         }
@@ -511,23 +544,24 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P) {
         if (levels_.empty() && first_P) {
             if (first_P->n != A.n || first_P->m <= 0 || first_P->m >= A.n)
                 throw Error(VG_EINVAL, "first multigrid prolongator does not fit the matrix");
-            L.omega = 4.0 / (3.0 * rho_dinv_a(A, L.dinv));
+            L.omega = 4.0 / (3.0 * rho_dinv_a(A, dinv_own));
             P = *first_P;
             nagg = P.m;
         } else {
             std::vector<int> agg = aggregate(A, theta, nagg);
             if (nagg >= A.n || nagg == 0) {  // no coarsening possible
+                if (fine) A = permute_csr(A, fine_order, fine_order);
                 levels_.push_back(std::move(L));
                 break;
             }
-            L.omega = 4.0 / (3.0 * rho_dinv_a(A, L.dinv));
-            P = smoothed_prolongator(A, agg, nagg, L.dinv, L.omega);
+            L.omega = 4.0 / (3.0 * rho_dinv_a(A, dinv_own));
+            P = smoothed_prolongator(A, agg, nagg, dinv_own, L.omega);
         }
         HostCsr R = transpose(P);
         HostCsr Ac = spgemm(R, spgemm(A, P));
         L.nc = nagg;
-        to_sell(P, L.P, false);
-        to_sell(R, L.R, false);
+        to_sell(fine ? permute_csr(P, fine_order, nullptr) : P, L.P, false);
+        to_sell(fine ? permute_csr(R, nullptr, fine_order) : R, L.R, false);
         levels_.push_back(std::move(L));
         A = std::move(Ac);
         pt.mark("multigrid level (host)");

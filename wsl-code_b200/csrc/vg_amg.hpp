@@ -46,8 +46,10 @@ constexpr int COARSE_MAX = 2500;
 class Amg {
 public:
     // build the hierarchy of S (host CSR, symmetric positive definite or semi-definite); first_P, when
-    // given, is the prolongator of the finest level (no aggregation there)
-    void setup(const HostCsr& S, const HostCsr* first_P);
+    // given, is the prolongator of the finest level (no aggregation there); fine_order, when given,
+    // renumbers the finest level's rows for the vectors the cycle acts on (row i -> fine_order[i])
+    // after S has been coarsened in its own order
+    void setup(const HostCsr& S, const HostCsr* first_P, const std::vector<int>* fine_order = nullptr);
     bool ready() const { return !levels_.empty(); }
     int levels() const { return int(levels_.size()); }
     long long nnz() const;

@@ -158,7 +158,7 @@ struct SmemSrc {
 
 // one cell; K and NE compile-time. PRE: issue every operator load before the dependent gathers
 template <typename T, int K, int NE, bool PRE, class Src>
-__device__ __forceinline__ void cell_apply(const ApplyArgs<T>& a, const Src& src, int cell, double& quad,
+__device__ __forceinline__ void cell_apply(const ApplyArgs<T>& a, const Src& src, int prow, double& quad,
                                            double& msum) {
     constexpr int Q = (K + 1) * (K + 2) / 2, NI = Q - 1 + K * (K + 1) / 2, ED = (K + 1) * NE, N = ED + NI;
     constexpr int NPK = N * (N + 1) / 2;
@@ -171,7 +171,7 @@ __device__ __forceinline__ void cell_apply(const ApplyArgs<T>& a, const Src& src
     int g[N];
 #pragma unroll
     for (int i = 0; i < N; ++i) g[i] = src.g(i);
-    const long long pb = a.nf + (long long)cell * Q;
+    const long long pb = prow;
     T u[N], yu[N], pr[Q];
 #pragma unroll
     for (int i = 0; i < N; ++i) {
@@ -238,7 +238,7 @@ __device__ __forceinline__ void cell_apply(const ApplyArgs<T>& a, const Src& src
         T lam = a.x[a.N - 1];
 #pragma unroll
         for (int r = 0; r < Q; ++r) {
-            T l = a.L[(long long)cell * Q + r];
+            T l = a.L[(pb - a.nf) + r];
             yp[r] += l * lam;
             msum += double(l) * double(pr[r]);
         }
@@ -251,7 +251,7 @@ __device__ __forceinline__ void cell_apply(const ApplyArgs<T>& a, const Src& src
 // generic cell body: any k, any edge count up to MAX_NE, local arrays in thread-local memory
 constexpr int GEN_MAXN = 5 * MAX_NE + 24;
 template <typename T, class Src>
-__device__ void cell_apply_generic(const ApplyArgs<T>& a, const Src& src, int ne, int n, int cell, double& quad,
+__device__ void cell_apply_generic(const ApplyArgs<T>& a, const Src& src, int ne, int n, int prow, double& quad,
                                    double& msum) {
     const int K = a.k, Q = (K + 1) * (K + 2) / 2, ED = (K + 1) * ne, N = n;
     int g[GEN_MAXN];
@@ -265,7 +265,7 @@ __device__ void cell_apply_generic(const ApplyArgs<T>& a, const Src& src, int ne
         u[i] = gi < 0 ? -xv : xv;
         yu[i] = T(0);
     }
-    const long long pb = a.nf + (long long)cell * Q;
+    const long long pb = prow;
     for (int r = 0; r < Q; ++r) {
         pr[r] = a.x[pb + r];
         yp[r] = T(0);
@@ -308,7 +308,7 @@ __device__ void cell_apply_generic(const ApplyArgs<T>& a, const Src& src, int ne
     if (a.mult) {
         T lam = a.x[a.N - 1];
         for (int r = 0; r < Q; ++r) {
-            T l = a.L[(long long)cell * Q + r];
+            T l = a.L[(pb - a.nf) + r];
             yp[r] += l * lam;
             msum += double(l) * double(pr[r]);
         }
@@ -329,20 +329,20 @@ __device__ __forceinline__ void piece_global(const ApplyArgs<T>& a, const Piece&
                                              double& msum) {
     if (lane >= P.count) return;
     GlobalSrc<T> src{a.A + P.a_off + lane, a.W + P.w_off + lane, a.map + P.map_off + lane};
-    const int cell = __ldg(a.slot_cell + P.slot + lane);
+    const int prow = __ldg(a.prow + P.slot + lane);  // first pressure row of the cell
     if constexpr (K == 0 || K == 1) {
         switch (P.ne) {
-        case 3: cell_apply<T, K, 3, prefetch_all<K, 3>()>(a, src, cell, quad, msum); return;
-        case 4: cell_apply<T, K, 4, prefetch_all<K, 4>()>(a, src, cell, quad, msum); return;
-        case 5: cell_apply<T, K, 5, prefetch_all<K, 5>()>(a, src, cell, quad, msum); return;
-        case 6: cell_apply<T, K, 6, prefetch_all<K, 6>()>(a, src, cell, quad, msum); return;
-        case 7: cell_apply<T, K, 7, prefetch_all<K, 7>()>(a, src, cell, quad, msum); return;
-        case 8: cell_apply<T, K, 8, prefetch_all<K, 8>()>(a, src, cell, quad, msum); return;
-        case 9: cell_apply<T, K, 9, prefetch_all<K, 9>()>(a, src, cell, quad, msum); return;
+        case 3: cell_apply<T, K, 3, prefetch_all<K, 3>()>(a, src, prow, quad, msum); return;
+        case 4: cell_apply<T, K, 4, prefetch_all<K, 4>()>(a, src, prow, quad, msum); return;
+        case 5: cell_apply<T, K, 5, prefetch_all<K, 5>()>(a, src, prow, quad, msum); return;
+        case 6: cell_apply<T, K, 6, prefetch_all<K, 6>()>(a, src, prow, quad, msum); return;
+        case 7: cell_apply<T, K, 7, prefetch_all<K, 7>()>(a, src, prow, quad, msum); return;
+        case 8: cell_apply<T, K, 8, prefetch_all<K, 8>()>(a, src, prow, quad, msum); return;
+        case 9: cell_apply<T, K, 9, prefetch_all<K, 9>()>(a, src, prow, quad, msum); return;
         default: break;
         }
     }
-    cell_apply_generic<T>(a, src, P.ne, P.n, cell, quad, msum);
+    cell_apply_generic<T>(a, src, P.ne, P.n, prow, quad, msum);
 }
 
 // one lane of a piece record in shared memory: header int4 {ne, n, count, bytes}
@@ -354,16 +354,16 @@ __device__ __forceinline__ void piece_record(const ApplyArgs<T>& a, const unsign
     const T* A = reinterpret_cast<const T*>(r + 16) + lane;
     const int* m = reinterpret_cast<const int*>(reinterpret_cast<const T*>(r + 16) + (npk + nw) * PIECE) + lane;
     SmemSrc<T> src{A, A + npk * PIECE, m};
-    const int cell = m[n * PIECE];
+    const int prow = m[n * PIECE];  // first pressure row of the cell
     switch (ne) {
-    case 3: cell_apply<T, K, 3, false>(a, src, cell, quad, msum); return;
-    case 4: cell_apply<T, K, 4, false>(a, src, cell, quad, msum); return;
-    case 5: cell_apply<T, K, 5, false>(a, src, cell, quad, msum); return;
-    case 6: cell_apply<T, K, 6, false>(a, src, cell, quad, msum); return;
-    case 7: cell_apply<T, K, 7, false>(a, src, cell, quad, msum); return;
-    case 8: cell_apply<T, K, 8, false>(a, src, cell, quad, msum); return;
-    case 9: cell_apply<T, K, 9, false>(a, src, cell, quad, msum); return;
-    default: cell_apply_generic<T>(a, src, ne, n, cell, quad, msum);
+    case 3: cell_apply<T, K, 3, false>(a, src, prow, quad, msum); return;
+    case 4: cell_apply<T, K, 4, false>(a, src, prow, quad, msum); return;
+    case 5: cell_apply<T, K, 5, false>(a, src, prow, quad, msum); return;
+    case 6: cell_apply<T, K, 6, false>(a, src, prow, quad, msum); return;
+    case 7: cell_apply<T, K, 7, false>(a, src, prow, quad, msum); return;
+    case 8: cell_apply<T, K, 8, false>(a, src, prow, quad, msum); return;
+    case 9: cell_apply<T, K, 9, false>(a, src, prow, quad, msum); return;
+    default: cell_apply_generic<T>(a, src, ne, n, prow, quad, msum);
     }
 }
 
@@ -526,7 +526,7 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? CTAS_PER_SM : 1) apply_
 
 template <typename T>
 __global__ void k_pack(const Piece* pieces, int np, const long long* rec_off, const T* A, const T* W, const int* map,
-                       const int* slot_cell, int k, unsigned char* out) {
+                       const int* prow, int k, unsigned char* out) {
     const int p = int((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (p >= np) return;
     const Piece P = pieces[p];
@@ -538,7 +538,7 @@ __global__ void k_pack(const Piece* pieces, int np, const long long* rec_off, co
     for (int j = 0; j < nw; ++j) As[(npk + j) * PIECE + lane] = W[P.w_off + (long long)j * PIECE + lane];
     int* m = reinterpret_cast<int*>(As + (npk + nw) * PIECE);
     for (int i = 0; i < n; ++i) m[i * PIECE + lane] = map[P.map_off + (long long)i * PIECE + lane];
-    m[n * PIECE + lane] = slot_cell[P.slot + lane];
+    m[n * PIECE + lane] = prow[P.slot + lane];
 }
 
 }  // namespace
@@ -622,9 +622,9 @@ StreamPlan plan_stream(const std::vector<Piece>& pieces, int k, int elem_bytes, 
 
 template <typename T>
 void pack_stream(const Piece* pieces, int npieces, const long long* rec_off, const T* A, const T* W, const int* map,
-                 const int* slot_cell, int k, unsigned char* out, cudaStream_t s) {
+                 const int* prow, int k, unsigned char* out, cudaStream_t s) {
     if (npieces == 0) return;
-    k_pack<T><<<(npieces * 32 + 255) / 256, 256, 0, s>>>(pieces, npieces, rec_off, A, W, map, slot_cell, k, out);
+    k_pack<T><<<(npieces * 32 + 255) / 256, 256, 0, s>>>(pieces, npieces, rec_off, A, W, map, prow, k, out);
     VG_CUDA(cudaGetLastError());
 }
 

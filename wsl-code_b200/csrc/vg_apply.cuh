@@ -23,11 +23,11 @@ struct ApplyArgs {
     T* y;               // flux edge entries must be zero on entry (atomic scatter)
     const T* A;         // packed A_E, piece layout
     const T* W;         // W_E (k >= 1), piece layout
-    const int* map;     // signed flux dof map, piece layout
-    const int* slot_cell;
+    const int* map;     // signed flux dof map, piece layout (indices of the vectors' order)
+    const int* prow;    // per slot: first pressure row of the cell (nf + rank * q), -1 on padding
     const Piece* pieces;
     int npieces, k;
-    const T* L;         // multiplier vector per cell (q), when mult
+    const T* L;         // multiplier vector, indexed like the pressure rows minus nf, when mult
     const int* mask;    // essential-BC mask (N), when constrained
     const int* flags;   // optional: skip when flags[0] != 0
     long long nf, N;
@@ -38,7 +38,7 @@ struct ApplyArgs {
     double* red;        // optional: quadratic form x^T K x -> red[0]
     // record stream (k <= 1): per piece one contiguous record
     //   int4 {ne, n, count, record bytes} | A_E (n(n+1)/2 x 32 T) | W_E (q n x 32 T, k >= 1)
-    //   | map (n x 32 int) | slot cell (32 int)
+    //   | map (n x 32 int) | pressure row (32 int)
     // streamed through a ring of shared-memory stages by cp.async.bulk; null: strided kernel
     const unsigned char* rec;
     const ApplyBatch* batches;
@@ -65,7 +65,7 @@ long long record_bytes(const Piece& P, int k, int elem_bytes);
 // write the records of all pieces (one warp per piece)
 template <typename T>
 void pack_stream(const Piece* pieces, int npieces, const long long* rec_off, const T* A, const T* W, const int* map,
-                 const int* slot_cell, int k, unsigned char* out, cudaStream_t s);
+                 const int* prow, int k, unsigned char* out, cudaStream_t s);
 // raise the dynamic shared-memory limit of the streamed kernels (outside any stream capture)
 void prepare_stream_kernels();
 

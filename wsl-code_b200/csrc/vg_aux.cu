@@ -206,6 +206,13 @@ __global__ void k_assemble_mask(const int* mask, long long N, const long long* r
         }
 }
 
+// out[j] = in[idx[j + off] - off]: a permutation of a vector (off = 0) or of its part from off on
+template <typename T>
+__global__ void k_gather(const T* in, const int* idx, long long off, T* out, long long n) {
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x)
+        out[j] = in[idx[j + off] - off];
+}
+
 __global__ void k_axpy64(double* x, const double* d, double a, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         x[i] += a * d[i];
@@ -270,6 +277,16 @@ void assemble_values(const double* A, const double* W, const int* map, const int
         VG_CUDA(cudaGetLastError());
     }
 }
+
+template <typename T>
+void gather_launch(const T* in, const int* idx, long long off, T* out, long long n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_gather<T><<<148 * 4, 256, 0, s>>>(in, idx, off, out, n);
+    VG_CUDA(cudaGetLastError());
+}
+template void gather_launch<double>(const double*, const int*, long long, double*, long long, cudaStream_t);
+template void gather_launch<float>(const float*, const int*, long long, float*, long long, cudaStream_t);
+template void gather_launch<int>(const int*, const int*, long long, int*, long long, cudaStream_t);
 
 void axpy64_kernel_launch(double* x, const double* d, double a, long long n, cudaStream_t s) {
     k_axpy64<<<148 * 4, 256, 0, s>>>(x, d, a, n);

@@ -139,15 +139,39 @@ int vg_apply(vg_handle* h, const void* x, void* y, int precision, int constraine
         if (!s.built) throw vg::Error(VG_ESTATE, "vg_build must run before vg_apply");
         if (!x || !y || x == y) throw vg::Error(VG_EINVAL, "apply requires distinct non-null vectors");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const bool internal = (precision & VG_ORDER_INTERNAL) != 0;
+        precision &= ~VG_ORDER_INTERNAL;
         if (precision == VG_FP64) {
             VG_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * s.N, st));
-            s.apply64(static_cast<const double*>(x), static_cast<double*>(y), constrained != 0, 1.0, st);
+            if (internal)
+                s.apply_int<double>(static_cast<const double*>(x), static_cast<double*>(y), constrained != 0, 1.0, st,
+                                    nullptr);
+            else
+                s.apply64(static_cast<const double*>(x), static_cast<double*>(y), constrained != 0, 1.0, st);
         } else if (precision == VG_FP32) {
             VG_CUDA(cudaMemsetAsync(y, 0, sizeof(float) * s.N, st));
-            s.apply32(static_cast<const float*>(x), static_cast<float*>(y), constrained != 0, 1.0f, st);
+            if (internal)
+                s.apply_int<float>(static_cast<const float*>(x), static_cast<float*>(y), constrained != 0, 1.0f, st,
+                                   nullptr);
+            else
+                s.apply32(static_cast<const float*>(x), static_cast<float*>(y), constrained != 0, 1.0f, st);
         } else {
             throw vg::Error(VG_EINVAL, "precision must be VG_FP64 or VG_FP32");
         }
+    });
+}
+
+int vg_permute(vg_handle* h, int to_internal, const void* in, void* out, int precision, void* stream) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!s.built) throw vg::Error(VG_ESTATE, "vg_build must run before vg_permute");
+        if (!in || !out || in == out) throw vg::Error(VG_EINVAL, "permute requires distinct non-null vectors");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (precision == VG_FP64)
+            s.permute<double>(static_cast<const double*>(in), static_cast<double*>(out), to_internal != 0, st);
+        else if (precision == VG_FP32)
+            s.permute<float>(static_cast<const float*>(in), static_cast<float*>(out), to_internal != 0, st);
+        else
+            throw vg::Error(VG_EINVAL, "precision must be VG_FP64 or VG_FP32");
     });
 }
 

@@ -25,6 +25,8 @@ void assemble_values(const double* A, const double* W, const int* map, const int
                      const double* L, const Piece* pieces, int npieces, int k, long long nf, long long N,
                      int constrained, int mult, const long long* rp, const int* ci, double* val, int* bad,
                      cudaStream_t s);
+template <typename T>
+void gather_launch(const T* in, const int* idx, long long off, T* out, long long n, cudaStream_t s);
 void contract_adjoint(const double* A, const int* map, const int* slot_cell, const int* mask, const Piece* pieces,
                       int npieces, int k, const double* x, const double* mu, int constrained, double* g,
                       cudaStream_t s);
@@ -255,6 +257,7 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
     d_cell_slot_.upload(cell_slot_);
     d_pieces_.upload(pieces_);
     d_map_.upload(map_host_);
+    plan_internal_order();
     pt.mark("uploads");
     plan_streams();
     pt.mark("record-stream plan");
@@ -292,6 +295,64 @@ void Solver::destroy_graphs() {
         graph_[p] = nullptr;
     }
 }
+
+void Solver::plan_internal_order() {
+    const long long NN = (long long)nf + np + 1;  // + the multiplier row, which keeps its index
+    e2i_host_.assign(NN, -1);
+    i2e_host_.assign(NN, -1);
+    map_int_host_.assign(map_host_.size(), 0);
+    prow_host_.assign(slot_cell_.size(), -1);
+    int nextf = 0, nextp = 0;
+    for (const auto& P : pieces_) {
+        for (int i = 0; i < P.n; ++i)
+            for (int j = 0; j < P.count; ++j) {
+                const long long o = P.map_off + (long long)i * PIECE + j;
+                const int g = map_host_[o], gg = g < 0 ? ~g : g;
+                if (e2i_host_[gg] < 0) {
+                    e2i_host_[gg] = nextf;
+                    i2e_host_[nextf] = gg;
+                    ++nextf;
+                }
+                const int gi = e2i_host_[gg];
+                map_int_host_[o] = g < 0 ? ~gi : gi;
+            }
+        for (int j = 0; j < P.count; ++j) {
+            const int c = slot_cell_[P.slot + j];
+            prow_host_[P.slot + j] = nf + nextp * q;
+            for (int r = 0; r < q; ++r) {
+                e2i_host_[nf + (long long)c * q + r] = nf + nextp * q + r;
+                i2e_host_[nf + (long long)nextp * q + r] = nf + c * q + r;
+            }
+            ++nextp;
+        }
+    }
+    e2i_host_[NN - 1] = int(NN - 1);
+    i2e_host_[NN - 1] = int(NN - 1);
+    if (nextf != nf || nextp != m.nc) throw Error(VG_EMESH, "dof numbering does not cover every unknown");
+    d_map_int_.upload(map_int_host_);
+    d_prow_.upload(prow_host_);
+    d_e2i_.upload(e2i_host_);
+    d_i2e_.upload(i2e_host_);
+}
+
+void Solver::internal_copies() {
+    d_mask_int_.resize(N);
+    gather_launch<int>(d_mask_.data(), d_i2e_.data(), 0, d_mask_int_.data(), N, nullptr);
+    d_Lint_.resize(size_t(np));
+    d_Lint32_.resize(size_t(np));
+    gather_launch<double>(d_L_.data(), d_i2e_.data(), nf, d_Lint_.data(), np, nullptr);
+    gather_launch<float>(d_L32_.data(), d_i2e_.data(), nf, d_Lint32_.data(), np, nullptr);
+    for (auto& b : d_pa64_) b.resize(N);
+    for (auto& b : d_pa32_) b.resize(N);
+    d_xi_.resize(N);
+}
+
+template <typename T>
+void Solver::permute(const T* in, T* out, bool to_internal, cudaStream_t s) {
+    gather_launch<T>(in, to_internal ? d_i2e_.data() : d_e2i_.data(), 0, out, N, s);
+}
+template void Solver::permute<double>(const double*, double*, bool, cudaStream_t);
+template void Solver::permute<float>(const float*, float*, bool, cudaStream_t);
 
 void Solver::pack_layout() {
     // chunks of CHUNK consecutive cells, grouped by edge count inside a chunk, split into pieces
@@ -468,6 +529,7 @@ void Solver::build() {
     for (const auto& c : classes_) launch_setup(a, c, nqp, nullptr);
     VG_CUDA(cudaDeviceSynchronize());
     check_status("setup");
+    internal_copies();
     pt.mark("device setup kernels");
     pack_streams(nullptr);
     pt.mark("pack record streams");
@@ -520,12 +582,24 @@ void Solver::make_diagonal(cudaStream_t s) {
     diag_invert(d_dinv64_.data(), bc == VG_BC_FLUX ? d_mask_.data() : nullptr, contrib.data(), m.nc, nf, np,
                 bc == VG_BC_FLUX, N, s);
     to_float_plain(d_dinv64_.data(), d_dinv32_.data(), N, s);
+    d_pdinv64_.resize(N);
+    d_pdinv32_.resize(N);
+    gather_launch<double>(d_dinv64_.data(), d_i2e_.data(), 0, d_pdinv64_.data(), N, s);
+    gather_launch<float>(d_dinv32_.data(), d_i2e_.data(), 0, d_pdinv32_.data(), N, s);
     VG_CUDA(cudaStreamSynchronize(s));
     // the captured Krylov loops hold the multigrid hierarchy's device addresses, which the rebuild
     // below frees: drop them (they are captured again by the next solve)
     destroy_graphs();
     use_amg = false;
     if (bc == VG_BC_PRESSURE) build_amg();
+}
+
+// pressure rows in the solver's internal order (index minus nf)
+std::vector<int> Solver::pressure_order() const {
+    std::vector<int> o;
+    o.resize(static_cast<size_t>(np));
+    for (long long i = 0; i < np; ++i) o[i] = e2i_host_[nf + i] - nf;
+    return o;
 }
 
 // pressure Schur block S = B diag(A)^{-1} B^T for k >= 1 (B[(E,r), g] = W_E[r,i] s_Ei over the local
@@ -625,7 +699,8 @@ void Solver::build_amg_high() {
             P0.ptr[c * q + r + 1] = int(P0.col.size());
         }
     try {
-        amg_.setup(S, &P0);
+        const std::vector<int> order = pressure_order();
+        amg_.setup(S, &P0, &order);
     } catch (const Error&) {
         use_amg = false;
         amg_levels = 0;
@@ -682,7 +757,8 @@ void Solver::build_amg() {
         S.ptr[c + 1] = int(S.col.size());
     }
     try {
-        amg_.setup(S, nullptr);
+        const std::vector<int> order = pressure_order();
+        amg_.setup(S, nullptr, &order);
     } catch (const Error&) {
         use_amg = false;  // diagonal preconditioner on the device
         amg_levels = 0;
@@ -693,16 +769,28 @@ void Solver::build_amg() {
     amg_setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
-void Solver::apply64(const double* x, double* y, bool constrained, double psign, cudaStream_t s, double* quad) {
-    launch_apply(apply_args<double>(x, y, constrained, psign, quad, nullptr), s);
+template <typename T>
+void Solver::apply_int(const T* x, T* y, bool constrained, T psign, cudaStream_t s, double* quad) {
+    launch_apply(apply_args<T>(x, y, constrained, psign, quad, nullptr), s);
     n_launch += 1;
     ++n_apply;
 }
+template void Solver::apply_int<double>(const double*, double*, bool, double, cudaStream_t, double*);
+template void Solver::apply_int<float>(const float*, float*, bool, float, cudaStream_t, double*);
+
+// reference order in and out: permute to the internal order, apply, permute back
+void Solver::apply64(const double* x, double* y, bool constrained, double psign, cudaStream_t s, double* quad) {
+    permute<double>(x, d_pa64_[0].data(), true, s);
+    VG_CUDA(cudaMemsetAsync(d_pa64_[1].data(), 0, sizeof(double) * N, s));
+    apply_int<double>(d_pa64_[0].data(), d_pa64_[1].data(), constrained, psign, s, quad);
+    permute<double>(d_pa64_[1].data(), y, false, s);
+}
 
 void Solver::apply32(const float* x, float* y, bool constrained, float psign, cudaStream_t s, double* quad) {
-    launch_apply(apply_args<float>(x, y, constrained, psign, quad, nullptr), s);
-    n_launch += 1;
-    ++n_apply;
+    permute<float>(x, d_pa32_[0].data(), true, s);
+    VG_CUDA(cudaMemsetAsync(d_pa32_[1].data(), 0, sizeof(float) * N, s));
+    apply_int<float>(d_pa32_[0].data(), d_pa32_[1].data(), constrained, psign, s, quad);
+    permute<float>(d_pa32_[1].data(), y, false, s);
 }
 
 void Solver::plan_streams() {
@@ -725,10 +813,10 @@ void Solver::plan_streams() {
 void Solver::pack_streams(cudaStream_t s) {
     if (k > 1) return;
     const int np_ = int(pieces_.size());
-    pack_stream<double>(d_pieces_.data(), np_, d_roff64_.data(), d_A64_.data(), d_W64_.data(), d_map_.data(),
-                        d_slot_cell_.data(), k, d_rec64_.data(), s);
-    pack_stream<float>(d_pieces_.data(), np_, d_roff32_.data(), d_A32_.data(), d_W32_.data(), d_map_.data(),
-                       d_slot_cell_.data(), k, d_rec32_.data(), s);
+    pack_stream<double>(d_pieces_.data(), np_, d_roff64_.data(), d_A64_.data(), d_W64_.data(), d_map_int_.data(),
+                        d_prow_.data(), k, d_rec64_.data(), s);
+    pack_stream<float>(d_pieces_.data(), np_, d_roff32_.data(), d_A32_.data(), d_W32_.data(), d_map_int_.data(),
+                       d_prow_.data(), k, d_rec32_.data(), s);
     VG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -751,13 +839,13 @@ void Solver::rhs(double* b, cudaStream_t s) {
 template <>
 MinresVecs<float> Solver::vecs<float>(float* x) {
     return MinresVecs<float>{w32_[0].data(), w32_[1].data(), w32_[2].data(), w32_[3].data(), w32_[4].data(),
-                             w32_[5].data(), w32_[6].data(), x, d_dinv32_.data()};
+                             w32_[5].data(), w32_[6].data(), x, d_pdinv32_.data()};
 }
 
 template <>
 MinresVecs<double> Solver::vecs<double>(double* x) {
     return MinresVecs<double>{w64_[0].data(), w64_[1].data(), w64_[2].data(), w64_[3].data(), w64_[4].data(),
-                              w64_[5].data(), w64_[6].data(), x, d_dinv64_.data()};
+                              w64_[5].data(), w64_[6].data(), x, d_pdinv64_.data()};
 }
 
 template <typename T>
@@ -768,18 +856,18 @@ ApplyArgs<T> Solver::apply_args(const T* x, T* y, bool constrained, T psign, dou
     if constexpr (sizeof(T) == 8) {
         a.A = d_A64_.data();
         a.W = d_W64_.data();
-        a.L = d_L_.data();
+        a.L = d_Lint_.data();
     } else {
         a.A = d_A32_.data();
         a.W = d_W32_.data();
-        a.L = d_L32_.data();
+        a.L = d_Lint32_.data();
     }
-    a.map = d_map_.data();
-    a.slot_cell = d_slot_cell_.data();
+    a.map = d_map_int_.data();
+    a.prow = d_prow_.data();
     a.pieces = d_pieces_.data();
     a.npieces = int(pieces_.size());
     a.k = k;
-    a.mask = d_mask_.data();
+    a.mask = d_mask_int_.data();
     a.flags = flags;
     a.nf = nf;
     a.N = N;
@@ -918,14 +1006,21 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
     const bool cons = bc == VG_BC_FLUX;
     // symmetric form: pressure / multiplier rows negated
     DevBuf<double>&bs = sv64_[0], &r = sv64_[1], &y = sv64_[2], &d = sv64_[3];
-    flip_pressure(b, bs.data(), nf, N, s);
-    n_launch += 1;
+    // the Krylov solve runs in the internal order: b and the initial x are permuted in, x out
+    double* const x_ext = x;
+    x = d_xi_.data();
+    permute<double>(b, bs.data(), true, s);
+    flip_pressure(bs.data(), bs.data(), nf, N, s);
+    n_launch += 2;
     ++n_solve;
-    if (!o.nonzero_guess) VG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
+    if (o.nonzero_guess)
+        permute<double>(x_ext, x, true, s);
+    else
+        VG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
     double h_red[2] = {0, 0};
     auto true_residual = [&]() {
         y.zero(s);
-        apply64(x, y.data(), cons, -1.0, s);
+        apply_int<double>(x, y.data(), cons, -1.0, s, nullptr);
         residual64(bs.data(), y.data(), r.data(), N, d_red_.data(), d_partials_.data(), d_counter_.data(), s);
         n_launch += 1;
         VG_CUDA(cudaMemcpyAsync(h_red, d_red_.data(), sizeof(h_red), cudaMemcpyDeviceToHost, s));
@@ -961,6 +1056,7 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
             rel = true_residual();
         }
     }
+    permute<double>(x, x_ext, false, s);
     VG_CUDA(cudaEventRecord(ev1_, s));
     VG_CUDA(cudaEventSynchronize(ev1_));
     check_pipeline();

@@ -87,6 +87,14 @@ public:
 
 private:
     void pack_layout();
+    void plan_internal_order();
+    std::vector<int> pressure_order() const;
+    void internal_copies();  // L, mask (after the setup) in the internal order
+public:
+    // y = K x with x, y in the internal order (y's flux entries zero on entry)
+    template <typename T>
+    void apply_int(const T* x, T* y, bool constrained, T psign, cudaStream_t s, double* quad);
+private:
     void plan_streams();
     void pack_streams(cudaStream_t s);
     void check_pipeline();
@@ -185,6 +193,18 @@ private:
     DevBuf<double> d_hb_, d_hx_;  // device copies of the host-buffer solve
     DevBuf<double> d_rhs0_;       // right-hand side before the essential-BC lift
     DevBuf<double> d_adj_rhs_, d_adj_mu_;  // adjoint right-hand side and solution
+    // internal order of the solver's vectors: flux dofs numbered by first touch in piece order (the
+    // dofs a cell owns are consecutive across the lanes of its piece), pressure rows in slot order;
+    // the public entry points keep the reference's order and permute at the boundary
+    std::vector<int> map_int_host_, prow_host_, e2i_host_, i2e_host_;
+    DevBuf<int> d_map_int_, d_prow_, d_e2i_, d_i2e_, d_mask_int_;
+    DevBuf<double> d_Lint_, d_pdinv64_, d_pa64_[2], d_xi_;
+    DevBuf<float> d_Lint32_, d_pdinv32_, d_pa32_[2];
+public:
+    // x (N) to or from the internal order
+    template <typename T>
+    void permute(const T* in, T* out, bool to_internal, cudaStream_t s);
+private:
 };
 
 }  // namespace vg

@@ -9,6 +9,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 LIB_PATH = os.path.join(HERE, "libvemgpu.so")
 HEADER = os.path.join(ROOT, "include", "vemgpu.h")
 
+ORDER_INTERNAL = 0x100
 VG_OK, VG_EINVAL, VG_EMESH, VG_EGEOMETRY, VG_ESINGULAR, VG_ECUDA, VG_ENOCONV, VG_ESTATE, VG_ENOMEM = range(9)
 GEOM = {"identity": 0, "sine": 1, "arcs": 2}
 PROBLEM = {"sincos": 1, "sinsin": 2, "annulus": 3}
@@ -69,6 +70,7 @@ def lib():
         L.vg_build.argtypes = [P]
         L.vg_apply.argtypes = [P, P, P, I, I, P]
         L.vg_rhs.argtypes = [P, P]
+        L.vg_permute.argtypes = [P, I, P, P, I, P]
         L.vg_default_solve_opts.argtypes = [ctypes.POINTER(VgSolveOpts)]
         L.vg_default_solve_opts.restype = None
         L.vg_solve.argtypes = [P, P, P, ctypes.POINTER(VgSolveOpts), ctypes.POINTER(VgSolveInfo)]

@@ -128,12 +128,25 @@ class DarcyGpu:
         torch = _torch()
         return torch.zeros(self.N, dtype=dtype or torch.float64, device="cuda")
 
-    def apply(self, x, constrained=True, out=None):
+    def apply(self, x, constrained=True, out=None, internal_order=False):
+        """y = K x (reference sign). internal_order: x and y in the solver's internal order (see
+        permute), no permutation at the boundary."""
         torch = _torch()
         prec = L.FP64 if x.dtype == torch.float64 else L.FP32
+        if internal_order:
+            prec |= L.ORDER_INTERNAL
         y = out if out is not None else torch.empty_like(x)
         stream = torch.cuda.current_stream().cuda_stream
         L.check(L.lib().vg_apply(self.h, x.data_ptr(), y.data_ptr(), prec, int(constrained), stream), self.h)
+        return y
+
+    def permute(self, x, to_internal=True):
+        """Vector in the reference order -> the solver's internal order (to_internal=False: back)."""
+        torch = _torch()
+        prec = L.FP64 if x.dtype == torch.float64 else L.FP32
+        y = torch.empty_like(x)
+        stream = torch.cuda.current_stream().cuda_stream
+        L.check(L.lib().vg_permute(self.h, int(to_internal), x.data_ptr(), y.data_ptr(), prec, stream), self.h)
         return y
 
     def rhs(self):
