@@ -195,3 +195,30 @@ def test_theta_update_rebuilds_multigrid(annulus2k):
         assert torch.linalg.norm(xa - xb) <= 1e-9 * torch.linalg.norm(xb)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("k,cells,domain", [(0, 30000, "annulus"), (1, 8000, "disk")])
+def test_multigrid_refresh_on_permeability_update(k, cells, domain):
+    """A permeability update recomputes the multigrid's values on the device (aggregates and
+    patterns kept): the solve matches a handle built from scratch with the new permeability."""
+    m = meshgen.voronoi_mesh(cells, domain, seed=81 + k)
+    cen = fields.cell_centroids(m)
+    th1 = fields.gaussian_field(cen, sigma=1.5, corr=0.1, seed=82)
+    th2 = fields.gaussian_field(cen, sigma=1.5, corr=0.1, seed=83)
+    geo = dict(geometry="arcs", problem="annulus" if domain == "annulus" else "sinsin", bc="pressure")
+    a = vemgpu.DarcyGpu(m, k=k, theta=th1, **geo)
+    x1, i1 = a.solve(tol=1e-10)
+    a.set_log_permeability(th1)  # same values through the refresh path
+    x1b, i1b = a.solve(tol=1e-10)
+    assert abs(i1b["iterations"] - i1["iterations"]) <= 2
+    assert torch.linalg.norm(x1b - x1) <= 1e-9 * torch.linalg.norm(x1)
+    a.set_log_permeability(th2)
+    b = vemgpu.DarcyGpu(m, k=k, theta=th2, **geo)
+    for mode in ("fp64", "mixed"):
+        xa, ia = a.solve(tol=1e-10, mode=mode)
+        xb, ib = b.solve(tol=1e-10, mode=mode)
+        assert ia["residual"] <= 1e-10
+        assert ia["iterations"] <= 1.3 * ib["iterations"] + 5, (ia, ib)
+        assert torch.linalg.norm(xa - xb) <= 1e-8 * torch.linalg.norm(xb)
+    a.close()
+    b.close()

@@ -17,6 +17,7 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 import vemgpu  # noqa: E402
+from vemgpu import default_nq  # noqa: E402
 from vemgpu import meshgen  # noqa: E402
 
 GEO = {O.GEOM_IDENTITY: "identity", O.GEOM_SINE: "sine", O.GEOM_ARCS: "arcs"}
@@ -25,6 +26,7 @@ BCN = {O.BC_FLUX: "flux", O.BC_PRESSURE: "pressure"}
 
 
 def pair(mesh, k, nq, geom, eps, problem, bc, theta=None, ng=9):
+    ng = max(ng, k + 2)
     o = O.Oracle(mesh, k=k, nq=nq, ng=ng, geom=geom, eps=eps, problem=problem, bc=bc, theta=theta)
     g = vemgpu.DarcyGpu(mesh, k=k, nq=nq, ng=ng, geometry=GEO[geom], eps=eps, problem=PROB[problem], bc=BCN[bc],
                         theta=theta)
@@ -306,3 +308,15 @@ def test_internal_order_apply_and_permute(disk200):
     y = g.apply(x)
     yi = g.apply(xi, internal_order=True)
     assert torch.equal(g.permute(yi, to_internal=False), y)
+
+
+@pytest.mark.parametrize("k", [2, 3])
+def test_multigrid_high_order_pressure_bc(k):
+    """k >= 2 with the pressure condition: the pressure block's multigrid starts from the
+    q-moment Schur block (injection of the cell means)."""
+    m = meshgen.voronoi_mesh(1500, "disk", seed=64 + k)
+    o, g = pair(m, k, default_nq(k), O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
+    xo, _, _ = o.solve_direct()
+    x, info = g.solve(tol=1e-10)
+    assert info["residual"] <= 1e-10
+    assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)

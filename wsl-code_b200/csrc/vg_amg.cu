@@ -42,6 +42,28 @@ HostCsr transpose(const HostCsr& A) {
     return T;
 }
 
+// transpose and, for every entry of the result, its position in A
+HostCsr transpose_map(const HostCsr& A, std::vector<int>& pos) {
+    HostCsr T;
+    T.n = A.m;
+    T.m = A.n;
+    T.ptr.assign(T.n + 1, 0);
+    for (int c : A.col) T.ptr[c + 1]++;
+    for (int i = 0; i < T.n; ++i) T.ptr[i + 1] += T.ptr[i];
+    T.col.resize(A.col.size());
+    T.val.resize(A.val.size());
+    pos.assign(A.col.size(), 0);
+    std::vector<int> fill(T.ptr.begin(), T.ptr.end() - 1);
+    for (int i = 0; i < A.n; ++i)
+        for (int j = A.ptr[i]; j < A.ptr[i + 1]; ++j) {
+            int d = fill[A.col[j]]++;
+            T.col[d] = i;
+            T.val[d] = A.val[j];
+            pos[d] = j;
+        }
+    return T;
+}
+
 HostCsr spgemm(const HostCsr& A, const HostCsr& B) {
     HostCsr C;
     C.n = A.n;
@@ -436,14 +458,122 @@ __global__ void k_gj_sym(const double* a, int n, double* o64, float* o32) {
     o32[t] = float(v);
 }
 
+// ---- numeric refresh of a hierarchy with fixed structure (one thread per row, fixed order) -------
+__device__ __forceinline__ int find_col(const int* col, int lo, int hi, int c) {
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (col[mid] < c)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;  // position of c when present
+}
+
+__global__ void k_diag_inv(const int* ptr, const int* col, const double* val, int n, double* d64, float* d32) {
+    int r = blockIdx.x * TPB + threadIdx.x;
+    if (r >= n) return;
+    int lo = ptr[r], hi = ptr[r + 1];
+    int j = find_col(col, lo, hi, r);
+    double v = (j < hi && col[j] == r) ? val[j] : 0.0;
+    double iv = v != 0.0 ? 1.0 / v : 0.0;
+    d64[r] = iv;
+    d32[r] = float(iv);
+}
+
+// P = (I - omega D^{-1} A) P_tent on the fixed pattern of P (rows in A's stored order)
+__global__ void k_smooth_p(const int* aptr, const int* acol, const double* aval, const int* agg, const double* dinv,
+                           double omega, const int* pptr, const int* pcol, double* pval, int n) {
+    int t = blockIdx.x * TPB + threadIdx.x;
+    if (t >= n) return;
+    const int lo = pptr[t], hi = pptr[t + 1];
+    for (int j = lo; j < hi; ++j) pval[j] = 0.0;
+    int j = find_col(pcol, lo, hi, agg[t]);
+    if (j < hi && pcol[j] == agg[t]) pval[j] += 1.0;
+    const double f = -omega * dinv[t];
+    for (int e = aptr[t]; e < aptr[t + 1]; ++e) {
+        const int J = agg[acol[e]];
+        j = find_col(pcol, lo, hi, J);
+        if (j < hi && pcol[j] == J) pval[j] += f * aval[e];
+    }
+}
+
+__global__ void k_take(const double* src, const int* map, double* dst, long long n) {
+    for (long long i = blockIdx.x * (long long)TPB + threadIdx.x; i < n; i += (long long)gridDim.x * TPB)
+        dst[i] = src[map[i]];
+}
+
+// C = R A P on C's fixed pattern, one coarse row per thread
+__global__ void k_rap(const int* rptr, const int* rcol, const double* rval, const int* aptr, const int* acol,
+                      const double* aval, const int* pptr, const int* pcol, const double* pval, const int* cptr,
+                      const int* ccol, double* cval, int nc) {
+    int I = blockIdx.x * TPB + threadIdx.x;
+    if (I >= nc) return;
+    const int lo = cptr[I], hi = cptr[I + 1];
+    for (int j = lo; j < hi; ++j) cval[j] = 0.0;
+    for (int u = rptr[I]; u < rptr[I + 1]; ++u) {
+        const int t = rcol[u];
+        const double rv = rval[u];
+        for (int e = aptr[t]; e < aptr[t + 1]; ++e) {
+            const int k = acol[e];
+            const double ra = rv * aval[e];
+            for (int w = pptr[k]; w < pptr[k + 1]; ++w) {
+                const int J = pcol[w];
+                const int j = find_col(ccol, lo, hi, J);
+                if (j < hi && ccol[j] == J) cval[j] += ra * pval[w];
+            }
+        }
+    }
+}
+
+__global__ void k_put_sell(const double* csr, const long long* pos, double* sell, long long n) {
+    for (long long i = blockIdx.x * (long long)TPB + threadIdx.x; i < n; i += (long long)gridDim.x * TPB)
+        sell[pos[i]] = csr[i];
+}
+
+__global__ void k_to32(const double* a, float* b, long long n) {
+    for (long long i = blockIdx.x * (long long)TPB + threadIdx.x; i < n; i += (long long)gridDim.x * TPB)
+        b[i] = float(a[i]);
+}
+
+// dense copy of a CSR matrix with the tiny diagonal shift of dense_of (one block)
+__global__ void k_csr_dense(const int* ptr, const int* col, const double* val, int n, double* d) {
+    __shared__ double tr[TPB];
+    double t = 0;
+    for (int r = threadIdx.x; r < n; r += TPB)
+        for (int j = ptr[r]; j < ptr[r + 1]; ++j) {
+            d[(long long)r * n + col[j]] += val[j];
+            if (col[j] == r) t += val[j];
+        }
+    tr[threadIdx.x] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int i = 0; i < TPB; ++i) s += tr[i];
+        tr[0] = s;
+    }
+    __syncthreads();
+    const double shift = 1e-12 * tr[0] / n;
+    for (int r = threadIdx.x; r < n; r += TPB) d[(long long)r * n + r] += shift;
+}
+
 inline int blocks(int n) { return (n + TPB - 1) / TPB; }
 
 }  // namespace
 
 void Amg::dense_inverse_device(const std::vector<double>& a, int n) {
-    DevBuf<double> d, col(n), row(n);
-    DevBuf<unsigned long long> bad(1);
+    DevBuf<double> d;
     d.upload(a);
+    dense_inverse_of(d.data(), n);
+}
+
+void Amg::dense_inverse_of(double* dd, int n) {
+    DevBuf<double> col(n), row(n);
+    DevBuf<unsigned long long> bad(1);
+    struct {
+        double* p;
+        double* data() { return p; }
+    } d{dd};
     bad.zero();
     const long long nn = (long long)n * n;
     const int nb = int((nn + TPB - 1) / TPB);
@@ -458,6 +588,50 @@ void Amg::dense_inverse_device(const std::vector<double>& a, int n) {
     unsigned long long b = 0;
     VG_CUDA(cudaMemcpy(&b, bad.data(), sizeof(b), cudaMemcpyDeviceToHost));
     if (b) throw Error(VG_ESINGULAR, "coarsest multigrid matrix is not positive definite");
+}
+
+void Amg::refresh(const double* a0) {
+    if (levels_.empty()) throw Error(VG_ESTATE, "multigrid refresh before setup");
+    const int nl = int(levels_.size());
+    const double* aval = a0;
+    for (int l = 0; l < nl; ++l) {
+        Level& L = levels_[l];
+        const long long nnz = (long long)L.pa_col.size();
+        if (L.A.csr) {
+            if (aval != L.cA_v64.data())
+                VG_CUDA(cudaMemcpy(L.cA_v64.data(), aval, sizeof(double) * nnz, cudaMemcpyDeviceToDevice));
+            k_to32<<<148 * 4, TPB>>>(L.cA_v64.data(), L.cA_v32.data(), nnz);
+        } else {
+            k_put_sell<<<148 * 4, TPB>>>(aval, L.dsellpos.data(), L.dA_v64.data(), nnz);
+            k_to32<<<148 * 4, TPB>>>(L.dA_v64.data(), L.dA_v32.data(), (long long)L.dA_v64.size());
+        }
+        k_diag_inv<<<blocks(L.n), TPB>>>(L.dpa_ptr.data(), L.dpa_col.data(), aval, L.n, L.dinv64.data(),
+                                         L.dinv32.data());
+        VG_CUDA(cudaGetLastError());
+        if (l == nl - 1) {  // coarsest: dense inverse of the refreshed matrix
+            DevBuf<double> d(size_t(L.n) * L.n);
+            d.zero();
+            k_csr_dense<<<1, TPB>>>(L.dpa_ptr.data(), L.dpa_col.data(), aval, L.n, d.data());
+            VG_CUDA(cudaGetLastError());
+            dense_inverse_of(d.data(), L.n);
+            break;
+        }
+        const long long pn = (long long)L.P.ccol.size(), rn = (long long)L.R.ccol.size();
+        if (!L.fixedP)
+            k_smooth_p<<<blocks(L.n), TPB>>>(L.dpa_ptr.data(), L.dpa_col.data(), aval, L.dagg.data(), L.dinv64.data(),
+                                             L.omega, L.cP_ptr.data(), L.cP_col.data(), L.cP_v64.data(), L.n);
+        k_take<<<148 * 4, TPB>>>(L.cP_v64.data(), L.dr2p.data(), L.cR_v64.data(), rn);
+        k_to32<<<148 * 4, TPB>>>(L.cP_v64.data(), L.cP_v32.data(), pn);
+        k_to32<<<148 * 4, TPB>>>(L.cR_v64.data(), L.cR_v32.data(), rn);
+        Level& C = levels_[l + 1];
+        if (!C.A.csr) throw Error(VG_ESTATE, "multigrid refresh: coarse operator not in CSR storage");
+        k_rap<<<blocks(L.nc), TPB>>>(L.cR_ptr.data(), L.cR_col.data(), L.cR_v64.data(), L.dpa_ptr.data(),
+                                      L.dpa_col.data(), aval, L.cP_ptr.data(), L.cP_col.data(), L.cP_v64.data(),
+                                      C.cA_ptr.data(), C.cA_col.data(), C.cA_v64.data(), L.nc);
+        VG_CUDA(cudaGetLastError());
+        aval = C.cA_v64.data();
+    }
+    VG_CUDA(cudaDeviceSynchronize());
 }
 
 long long Amg::nnz() const {
@@ -528,11 +702,19 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
         // order) and stored in fine_order, the order of the vectors it will act on
         const bool fine = levels_.empty() && fine_order;
         const std::vector<double> dinv_own(L.dinv);  // in A's own order (smoothing, spectral radius)
-        if (fine) {
-            for (int i = 0; i < A.n; ++i) L.dinv[(*fine_order)[i]] = dinv_own[i];
-            to_sell(permute_csr(A, fine_order, fine_order), L.A, true);
-        } else {
-            to_sell(A, L.A, levels_.empty());
+        {
+            HostCsr Ast = fine ? permute_csr(A, fine_order, fine_order) : A;
+            if (fine)
+                for (int i = 0; i < A.n; ++i) L.dinv[(*fine_order)[i]] = dinv_own[i];
+            to_sell(Ast, L.A, levels_.empty());
+            L.pa_ptr = Ast.ptr;
+            L.pa_col = Ast.col;
+            if (!L.A.csr) {
+                L.sellpos.resize(Ast.col.size());
+                for (int r = 0; r < Ast.n; ++r)
+                    for (int j = Ast.ptr[r]; j < Ast.ptr[r + 1]; ++j)
+                        L.sellpos[j] = L.A.soff[r / 32] + 32LL * (j - Ast.ptr[r]) + r % 32;
+            }
         }
         if (A.n <= COARSE_MAX || levels_.size() >= 16) {
             if (fine) A = permute_csr(A, fine_order, fine_order);
@@ -547,6 +729,7 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
             L.omega = 4.0 / (3.0 * rho_dinv_a(A, dinv_own));
             P = *first_P;
             nagg = P.m;
+            L.fixedP = true;
         } else {
             std::vector<int> agg = aggregate(A, theta, nagg);
             if (nagg >= A.n || nagg == 0) {  // no coarsening possible
@@ -556,12 +739,18 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
             }
             L.omega = 4.0 / (3.0 * rho_dinv_a(A, dinv_own));
             P = smoothed_prolongator(A, agg, nagg, dinv_own, L.omega);
+            L.agg.resize(A.n);
+            for (int i = 0; i < A.n; ++i) L.agg[fine ? (*fine_order)[i] : i] = agg[i];
         }
         HostCsr R = transpose(P);
         HostCsr Ac = spgemm(R, spgemm(A, P));
         L.nc = nagg;
-        to_sell(fine ? permute_csr(P, fine_order, nullptr) : P, L.P, false);
-        to_sell(fine ? permute_csr(R, nullptr, fine_order) : R, L.R, false);
+        {
+            HostCsr Pst = fine ? permute_csr(P, fine_order, nullptr) : P;
+            HostCsr Rst = transpose_map(Pst, L.r2p);
+            to_sell(Pst, L.P, false);
+            to_sell(Rst, L.R, false);
+        }
         levels_.push_back(std::move(L));
         A = std::move(Ac);
         pt.mark("multigrid level (host)");
@@ -609,6 +798,11 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
             v32.upload(f);
         };
         upc(L.A, L.cA_ptr, L.cA_col, L.cA_v64, L.cA_v32);
+        L.dpa_ptr.upload(L.pa_ptr);
+        L.dpa_col.upload(L.pa_col);
+        if (!L.agg.empty()) L.dagg.upload(L.agg);
+        if (!L.r2p.empty()) L.dr2p.upload(L.r2p);
+        if (!L.sellpos.empty()) L.dsellpos.upload(L.sellpos);
         upc(L.P, L.cP_ptr, L.cP_col, L.cP_v64, L.cP_v32);
         upc(L.R, L.cR_ptr, L.cR_col, L.cR_v64, L.cR_v32);
         L.dinv64.upload(L.dinv);

@@ -57,6 +57,14 @@ public:
     void vcycle(const double* b, double* z, cudaStream_t s);
     void vcycle(const float* b, float* z, cudaStream_t s);
     long long launches = 0;
+    // Recompute every value of the hierarchy on the device for a new finest-level operator with the
+    // same sparsity: the aggregates, sparsity patterns and smoothing weights of setup() are kept
+    // (a valid multigrid for any values; the captured cycle's device addresses do not change).
+    // a0: the finest level's values in the order of its stored pattern (level0_ptr / level0_col).
+    void refresh(const double* a0);
+    const int* level0_ptr() const { return levels_.empty() ? nullptr : levels_[0].dpa_ptr.data(); }
+    const int* level0_col() const { return levels_.empty() ? nullptr : levels_[0].dpa_col.data(); }
+    long long level0_nnz() const { return levels_.empty() ? 0 : (long long)levels_[0].pa_col.size(); }
 
 private:
     struct Sell {
@@ -75,6 +83,14 @@ private:
         double omega = 0;
         Sell A, P, R;  // P: n x nc, R = P^T: nc x n (absent on the coarsest level)
         std::vector<double> dinv;
+        // structure kept for refresh(): stored CSR pattern of A, aggregate of every stored row (empty
+        // when the prolongator is given), position in P of every R entry, SELL slot of every CSR
+        // entry of A (SELL storage)
+        std::vector<int> pa_ptr, pa_col, agg, r2p;
+        std::vector<long long> sellpos;
+        bool fixedP = false;
+        DevBuf<int> dpa_ptr, dpa_col, dagg, dr2p;
+        DevBuf<long long> dsellpos;
         // device
         DevBuf<long long> dA_soff, dP_soff, dR_soff;
         DevBuf<int> dA_w, dA_col, dP_w, dP_col, dR_w, dR_col;
@@ -87,6 +103,7 @@ private:
     template <typename T>
     void cycle(int l, const T* b, T* z, cudaStream_t s);
     void dense_inverse_device(const std::vector<double>& a, int n);
+    void dense_inverse_of(double* d, int n);  // in-place device matrix -> dinvc64_ / dinvc32_
     template <typename T>
     DevSell<T> view(const Level& L, int which) const;
     template <typename T>

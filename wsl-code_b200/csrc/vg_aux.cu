@@ -206,6 +206,48 @@ __global__ void k_assemble_mask(const int* mask, long long N, const long long* r
         }
 }
 
+// values of the pressure Schur block S = B diag(A)^{-1} B^T on its stored pattern (rows and columns
+// in the solver's internal pressure order): row (E, r) sums over the flux dofs g of E, over the cells
+// F around g and the moments r2 of F: W_E[r, i] s_Ei dinv[g] W_F[r2, j] s_Fj (k = 0: W = 1)
+__global__ void k_schur_values(const int* sptr, const int* scol, int nrows, int q, int k, const int* rank_cell,
+                               const int* cell_rank, const int* cell_slot, const Piece* pieces, const int* map,
+                               const double* W, const double* dinv, const int* inc_ptr, const int* inc_cell,
+                               const int* inc_i, const signed char* inc_s, double* sval) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nrows) return;
+    const int c = rank_cell[t / q], r = t % q;
+    const int lo = sptr[t], hi = sptr[t + 1];
+    for (int j = lo; j < hi; ++j) sval[j] = 0.0;
+    const int slot = cell_slot[c];
+    const Piece P = pieces[slot / PIECE];
+    const int lane = slot % PIECE;
+    for (int i = 0; i < P.n; ++i) {
+        const int g0 = map[P.map_off + (long long)i * PIECE + lane], g = g0 < 0 ? ~g0 : g0;
+        const double wi = k == 0 ? 1.0 : W[P.w_off + (long long)(r * P.n + i) * PIECE + lane];
+        const double coef = wi * (g0 < 0 ? -1.0 : 1.0) * dinv[g];
+        if (coef == 0.0) continue;
+        for (int b = inc_ptr[g]; b < inc_ptr[g + 1]; ++b) {
+            const int F = inc_cell[b], jf = inc_i[b];
+            const int fslot = cell_slot[F];
+            const Piece Q = pieces[fslot / PIECE];
+            const int flane = fslot % PIECE;
+            for (int r2 = 0; r2 < q; ++r2) {
+                const int colv = cell_rank[F] * q + r2;
+                const double wf = k == 0 ? 1.0 : W[Q.w_off + (long long)(r2 * Q.n + jf) * PIECE + flane];
+                int a = lo, z = hi;
+                while (a < z) {
+                    int mid = (a + z) >> 1;
+                    if (scol[mid] < colv)
+                        a = mid + 1;
+                    else
+                        z = mid;
+                }
+                if (a < hi && scol[a] == colv) sval[a] += coef * wf * double(inc_s[b]);
+            }
+        }
+    }
+}
+
 // out[j] = in[idx[j + off] - off]: a permutation of a vector (off = 0) or of its part from off on
 template <typename T>
 __global__ void k_gather(const T* in, const int* idx, long long off, T* out, long long n) {
@@ -276,6 +318,14 @@ void assemble_values(const double* A, const double* W, const int* map, const int
         k_assemble_mask<<<148 * 4, 256, 0, s>>>(mask, N, rp, ci, val, bad);
         VG_CUDA(cudaGetLastError());
     }
+}
+
+void schur_values(const int* sptr, const int* scol, int nrows, int q, int k, const int* rank_cell, const int* cell_rank,
+                  const int* cell_slot, const Piece* pieces, const int* map, const double* W, const double* dinv,
+                  const int* inc_ptr, const int* inc_cell, const int* inc_i, const signed char* inc_s, double* sval) {
+    k_schur_values<<<(nrows + 255) / 256, 256>>>(sptr, scol, nrows, q, k, rank_cell, cell_rank, cell_slot, pieces, map, W,
+                                                 dinv, inc_ptr, inc_cell, inc_i, inc_s, sval);
+    VG_CUDA(cudaGetLastError());
 }
 
 template <typename T>

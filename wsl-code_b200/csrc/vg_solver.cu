@@ -27,6 +27,9 @@ void assemble_values(const double* A, const double* W, const int* map, const int
                      cudaStream_t s);
 template <typename T>
 void gather_launch(const T* in, const int* idx, long long off, T* out, long long n, cudaStream_t s);
+void schur_values(const int* sptr, const int* scol, int nrows, int q, int k, const int* rank_cell, const int* cell_rank,
+                  const int* cell_slot, const Piece* pieces, const int* map, const double* W, const double* dinv,
+                  const int* inc_ptr, const int* inc_cell, const int* inc_i, const signed char* inc_s, double* sval);
 void contract_adjoint(const double* A, const int* map, const int* slot_cell, const int* mask, const Piece* pieces,
                       int npieces, int k, const double* x, const double* mu, int constrained, double* g,
                       cudaStream_t s);
@@ -547,6 +550,7 @@ void Solver::build() {
     destroy_graphs();
     for (auto& b : sv64_) b.resize(N);
     for (auto& b : sv32_) b.resize(N);
+    amg_refreshable_ = false;  // a build starts the multigrid from scratch (the system may have changed)
     make_diagonal(nullptr);
     pt.mark("preconditioner (incl. multigrid)");
     // BC_FLUX: lifted right-hand side of MixedGpu::make_rhs (equation_gpu.cu:611-625):
@@ -587,11 +591,70 @@ void Solver::make_diagonal(cudaStream_t s) {
     gather_launch<double>(d_dinv64_.data(), d_i2e_.data(), 0, d_pdinv64_.data(), N, s);
     gather_launch<float>(d_dinv32_.data(), d_i2e_.data(), 0, d_pdinv32_.data(), N, s);
     VG_CUDA(cudaStreamSynchronize(s));
+    if (use_amg && amg_refreshable_) {
+        // new operator values on the kept structure: device refresh, same device addresses (the
+        // captured Krylov loops stay valid)
+        refresh_amg();
+        return;
+    }
     // the captured Krylov loops hold the multigrid hierarchy's device addresses, which the rebuild
     // below frees: drop them (they are captured again by the next solve)
     destroy_graphs();
     use_amg = false;
+    amg_refreshable_ = false;
     if (bc == VG_BC_PRESSURE) build_amg();
+    if (use_amg) prepare_amg_refresh();
+}
+
+// device arrays of the Schur values kernel: cells around every flux dof, cell <-> pressure rank
+void Solver::prepare_amg_refresh() {
+    std::vector<int> cnt(nf + 1, 0);
+    for (int c = 0; c < m.nc; ++c) {
+        const int slot = cell_slot_[c];
+        const Piece& P = pieces_[slot / PIECE];
+        for (int i = 0; i < P.n; ++i) {
+            int g = map_host_[P.map_off + (long long)i * PIECE + slot % PIECE];
+            cnt[(g < 0 ? ~g : g) + 1]++;
+        }
+    }
+    for (int g = 0; g < nf; ++g) cnt[g + 1] += cnt[g];
+    std::vector<int> icell(cnt[nf]), ii(cnt[nf]);
+    std::vector<signed char> is(cnt[nf]);
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (int c = 0; c < m.nc; ++c) {
+        const int slot = cell_slot_[c];
+        const Piece& P = pieces_[slot / PIECE];
+        for (int i = 0; i < P.n; ++i) {
+            int g = map_host_[P.map_off + (long long)i * PIECE + slot % PIECE], gg = g < 0 ? ~g : g;
+            icell[fill[gg]] = c;
+            ii[fill[gg]] = i;
+            is[fill[gg]++] = g < 0 ? -1 : 1;
+        }
+    }
+    std::vector<int> rank_cell(m.nc), cell_rank(m.nc);
+    for (int c = 0; c < m.nc; ++c) {
+        const int rank = (e2i_host_[nf + (long long)c * q] - nf) / q;
+        cell_rank[c] = rank;
+        rank_cell[rank] = c;
+    }
+    d_inc_ptr_.upload(cnt);
+    d_inc_cell_.upload(icell);
+    d_inc_i_.upload(ii);
+    d_inc_s_.upload(is);
+    d_rank_cell_.upload(rank_cell);
+    d_cell_rank_.upload(cell_rank);
+    d_schur_vals_.resize(size_t(amg_.level0_nnz()));
+    amg_refreshable_ = amg_.level0_nnz() > 0;
+}
+
+void Solver::refresh_amg() {
+    auto t0 = std::chrono::steady_clock::now();
+    VG_CUDA(cudaDeviceSynchronize());
+    schur_values(amg_.level0_ptr(), amg_.level0_col(), int(np), q, k, d_rank_cell_.data(), d_cell_rank_.data(),
+                 d_cell_slot_.data(), d_pieces_.data(), d_map_.data(), d_W64_.data(), d_dinv64_.data(),
+                 d_inc_ptr_.data(), d_inc_cell_.data(), d_inc_i_.data(), d_inc_s_.data(), d_schur_vals_.data());
+    amg_.refresh(d_schur_vals_.data());
+    amg_setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // pressure rows in the solver's internal order (index minus nf)

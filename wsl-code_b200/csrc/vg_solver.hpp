@@ -102,6 +102,12 @@ private:
     void lift_flux_rhs();
     void build_amg();
     void build_amg_high();
+    void prepare_amg_refresh();
+    void refresh_amg();
+    bool amg_refreshable_ = false;
+    DevBuf<int> d_inc_ptr_, d_inc_cell_, d_inc_i_, d_rank_cell_, d_cell_rank_;
+    DevBuf<signed char> d_inc_s_;
+    DevBuf<double> d_schur_vals_;
     template <typename T>
     void ms_precond(const T* r, T* z);
     template <typename T>
