@@ -427,7 +427,8 @@ __global__ void k_gj_save(const double* a, int n, int k, double* col, double* ro
     }
 }
 
-__global__ void k_gj_step(double* a, int n, int k, const double* col, const double* row, unsigned long long* bad) {
+__global__ void k_gj_step(double* a, int n, int k, const double* col, const double* row, unsigned long long* bad,
+                          double* ncol, double* nrow) {
     long long t = blockIdx.x * (long long)TPB + threadIdx.x;
     if (t >= (long long)n * n) return;
     const int i = int(t / n), j = int(t % n);
@@ -446,6 +447,11 @@ __global__ void k_gj_step(double* a, int n, int k, const double* col, const doub
     else
         v = a[t] - col[i] * row[j] / p;
     a[t] = v;
+    // the next step's saved column and row (ping-pong buffers): no separate save launch
+    if (ncol) {
+        if (j == k + 1) ncol[i] = v;
+        if (i == k + 1) nrow[j] = v;
+    }
 }
 
 // symmetric part in FP64 and FP32 (the exact inverse is symmetric)
@@ -577,9 +583,14 @@ void Amg::dense_inverse_of(double* dd, int n) {
     bad.zero();
     const long long nn = (long long)n * n;
     const int nb = int((nn + TPB - 1) / TPB);
+    DevBuf<double> col2(n), row2(n);
+    double *c0 = col.data(), *r0 = row.data(), *c1 = col2.data(), *r1 = row2.data();
+    k_gj_save<<<blocks(n), TPB>>>(d.data(), n, 0, c0, r0);
     for (int k = 0; k < n; ++k) {
-        k_gj_save<<<blocks(n), TPB>>>(d.data(), n, k, col.data(), row.data());
-        k_gj_step<<<nb, TPB>>>(d.data(), n, k, col.data(), row.data(), bad.data());
+        const bool more = k + 1 < n;
+        k_gj_step<<<nb, TPB>>>(d.data(), n, k, c0, r0, bad.data(), more ? c1 : nullptr, more ? r1 : nullptr);
+        std::swap(c0, c1);
+        std::swap(r0, r1);
     }
     dinvc64_.resize(size_t(nn));
     dinvc32_.resize(size_t(nn));
@@ -592,6 +603,7 @@ void Amg::dense_inverse_of(double* dd, int n) {
 
 void Amg::refresh(const double* a0) {
     if (levels_.empty()) throw Error(VG_ESTATE, "multigrid refresh before setup");
+    PhaseTimer pt;
     const int nl = int(levels_.size());
     const double* aval = a0;
     for (int l = 0; l < nl; ++l) {
@@ -613,7 +625,10 @@ void Amg::refresh(const double* a0) {
             d.zero();
             k_csr_dense<<<1, TPB>>>(L.dpa_ptr.data(), L.dpa_col.data(), aval, L.n, d.data());
             VG_CUDA(cudaGetLastError());
+            VG_CUDA(cudaDeviceSynchronize());
+            pt.mark("refresh: levels");
             dense_inverse_of(d.data(), L.n);
+            pt.mark("refresh: coarsest inverse");
             break;
         }
         const long long pn = (long long)L.P.ccol.size(), rn = (long long)L.R.ccol.size();

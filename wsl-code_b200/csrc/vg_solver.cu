@@ -444,9 +444,11 @@ void Solver::set_theta(const double* theta, bool on_device) {
     else
         VG_CUDA(cudaMemcpy(d_theta_.data(), theta, sizeof(double) * m.nc, cudaMemcpyHostToDevice));
     if (built) {
+        PhaseTimer pt;
         rescale_ops(d_theta_.data(), d_slot_cell_.data(), d_pieces_.data(), int(pieces_.size()), d_A0_.data(),
                     d_A64_.data(), d_A32_.data(), nullptr);
         pack_streams(nullptr);
+        pt.mark("rescale + record streams");
         make_diagonal(nullptr);
         lift_flux_rhs();
         VG_CUDA(cudaDeviceSynchronize());
@@ -594,7 +596,10 @@ void Solver::make_diagonal(cudaStream_t s) {
     if (use_amg && amg_refreshable_) {
         // new operator values on the kept structure: device refresh, same device addresses (the
         // captured Krylov loops stay valid)
+        PhaseTimer pt;
+        pt.mark("diagonal");
         refresh_amg();
+        pt.mark("multigrid refresh");
         return;
     }
     // the captured Krylov loops hold the multigrid hierarchy's device addresses, which the rebuild
