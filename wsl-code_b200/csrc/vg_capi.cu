@@ -274,6 +274,7 @@ int vg_ms_configure(vg_handle* h, double d12, double d13, double d23, double dt,
 int vg_ms_apply(vg_handle* h, const double* coeff_state, const void* x, void* y, int precision) {
     return guarded(h, [&](vg::Solver& s) {
         if (!coeff_state || !x || !y || x == y) throw vg::Error(VG_EINVAL, "null or aliased vector");
+        VG_CUDA(cudaDeviceSynchronize());  // inputs may come from any stream
         s.ms_coefficients(coeff_state);
         if (precision == VG_FP64)
             s.ms_apply(static_cast<const double*>(x), static_cast<double*>(y));

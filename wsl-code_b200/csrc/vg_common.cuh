@@ -127,6 +127,30 @@ constexpr int MAX_GL = 10;
 constexpr unsigned long long ST_SINGULAR = 1ull, ST_JACOBIAN = 2ull;
 
 #ifdef __CUDACC__
+// 16-byte vector access of 4 consecutive entries (the index is a multiple of 4 and every vector
+// starts on a cudaMalloc boundary): 4 floats in one load, 4 doubles in two
+__device__ __forceinline__ void ld4(const float* p, float (&o)[4]) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+    o[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&o)[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = b.x;
+    o[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
 __device__ __forceinline__ void set_status(unsigned long long* st, unsigned long long code, int cell) {
     atomicCAS(st, 0ull, (code << 40) | (unsigned long long)(unsigned)cell);
 }

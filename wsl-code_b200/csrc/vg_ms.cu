@@ -79,17 +79,17 @@ struct MsArgs {
     const int* mask; // boundary flux dofs (J.n = 0)
 };
 
-// y = K x; one lane per cell, both species; masked flux rows are identity rows
-template <typename T>
-__global__ void __launch_bounds__(MS_THREADS) k_ms_apply(MsArgs<T> a) {
-    Piece P;
-    int lane;
-    if (!ms_slot(a.pieces, a.npieces, P, lane)) return;
-    const int n = P.n;
+// one cell, both species (NE edges; NE = 0: runtime count up to MAX_NE, arrays in local memory)
+template <typename T, int NE>
+__device__ __forceinline__ void ms_cell(const MsArgs<T>& a, const Piece& P, int lane) {
+    constexpr int M = NE > 0 ? NE : MAX_NE;
+    const int n = NE > 0 ? NE : P.n;
     const int cell = a.slot_cell[P.slot + lane];
-    int g[MAX_NE];
-    T u0[MAX_NE], u1[MAX_NE], y0[MAX_NE], y1[MAX_NE];
-    for (int i = 0; i < n; ++i) {
+    int g[M];
+    T u0[M], u1[M], y0[M], y1[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        if (i >= n) break;
         int gi = a.map[P.map_off + (long long)i * PIECE + lane];
         g[i] = gi;
         int idx = gi < 0 ? ~gi : gi;
@@ -101,9 +101,14 @@ __global__ void __launch_bounds__(MS_THREADS) k_ms_apply(MsArgs<T> a) {
         y1[i] = T(0);
     }
     const T* Ap = a.A + P.a_off + lane;
-    for (int i = 0; i < n; ++i)
-        for (int c = i; c < n; ++c) {
-            const T v = Ap[(long long)packed_index(i, c, n) * PIECE];
+    int e = 0;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        if (i >= n) break;
+#pragma unroll
+        for (int c = i; c < M; ++c) {
+            if (c >= n) break;
+            const T v = Ap[(long long)(e++) * PIECE];
             y0[i] += v * u0[c];
             y1[i] += v * u1[c];
             if (c != i) {
@@ -111,11 +116,14 @@ __global__ void __launch_bounds__(MS_THREADS) k_ms_apply(MsArgs<T> a) {
                 y1[c] += v * u1[i];
             }
         }
+    }
     const T b00 = a.B[4LL * cell], b01 = a.B[4LL * cell + 1], b10 = a.B[4LL * cell + 2], b11 = a.B[4LL * cell + 3];
     const long long p0 = 2 * a.nf + cell, p1 = 2 * a.nf + a.nc + cell;
     const T pr0 = a.x[p0], pr1 = a.x[p1];
     T d0 = T(0), d1 = T(0);
-    for (int i = 0; i < n; ++i) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        if (i >= n) break;
         const int idx = g[i] < 0 ? ~g[i] : g[i];
         const T s = g[i] < 0 ? T(-1) : T(1);
         d0 += u0[i];
@@ -131,6 +139,33 @@ __global__ void __launch_bounds__(MS_THREADS) k_ms_apply(MsArgs<T> a) {
     const T m = a.mdt[cell];
     a.y[p0] = d0 + m * pr0;
     a.y[p1] = d1 + m * pr1;
+}
+
+// y = K x; one lane per cell, both species; masked flux rows are identity rows. Cells with 3..9
+// edges here (fixed-size register arrays), larger polygons in k_ms_apply_large
+template <typename T>
+__global__ void __launch_bounds__(MS_THREADS) k_ms_apply(MsArgs<T> a) {
+    Piece P;
+    int lane;
+    if (!ms_slot(a.pieces, a.npieces, P, lane)) return;
+    switch (P.n) {
+    case 3: ms_cell<T, 3>(a, P, lane); break;
+    case 4: ms_cell<T, 4>(a, P, lane); break;
+    case 5: ms_cell<T, 5>(a, P, lane); break;
+    case 6: ms_cell<T, 6>(a, P, lane); break;
+    case 7: ms_cell<T, 7>(a, P, lane); break;
+    case 8: ms_cell<T, 8>(a, P, lane); break;
+    case 9: ms_cell<T, 9>(a, P, lane); break;
+    default: break;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MS_THREADS) k_ms_apply_large(MsArgs<T> a) {
+    Piece P;
+    int lane;
+    if (!ms_slot(a.pieces, a.npieces, P, lane)) return;
+    if (P.n < 3 || P.n > 9) ms_cell<T, 0>(a, P, lane);
 }
 
 // preconditioner: assembled 2x2 flux blocks D_g = sum_E A_E,ii B_E (at most two addends per dof)
@@ -210,71 +245,265 @@ __global__ void k_ms_pc_apply(const T* r, T* z, const T* F, const T* C, long lon
     }
 }
 
-// partial dot products of w with the first cnt columns of V (column stride ld), one row of
-// MS_MAXM partials per block
-// (with self: w.w in slot cnt, cnt < MS_MAXM)
+// GMRES scalars on the device. The Arnoldi loop of one cycle runs as a CUDA graph (a conditional
+// while node around one iteration), so the Hessenberg column, the Givens rotations and the
+// residual estimate are formed on the device and the host reads them once per cycle.
+struct MsKrylov {
+    double H[MS_MAXM * MS_MAXM];  // H[i * MS_MAXM + c]: R factor of the Hessenberg matrix
+    double cs[MS_MAXM], sn[MS_MAXM], g[MS_MAXM + 1], y[MS_MAXM];
+    double hd[3 * MS_MAXM];  // [0, 32): first Gram-Schmidt pass, [32, 64): second, [64]: |w|^2, [65]: |t|^2
+    double beta0, tol, rel;
+    int j, its, m, maxit, done, pad_;
+};
+
+// one V-cycle-sized work split: block b owns rows [b chunk, (b + 1) chunk); chunk is a multiple of 4
 template <typename T>
-__global__ void __launch_bounds__(MS_THREADS) k_mdot(const T* V, long long ld, int cnt, const T* w, long long n,
-                                                     double* partials, int self) {
-    double acc[MS_MAXM];
-#pragma unroll
-    for (int k = 0; k < MS_MAXM; ++k) acc[k] = 0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const double wi = double(w[i]);
-#pragma unroll
-        for (int k = 0; k < MS_MAXM; ++k) {
-            if (k < cnt) acc[k] += double(V[k * ld + i]) * wi;
-            if (self && k == cnt) acc[k] += wi * wi;
-        }
-    }
-    cnt += self;
-    __shared__ double sh[MS_THREADS / 32][MS_MAXM];
-    const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
-#pragma unroll
-    for (int k = 0; k < MS_MAXM; ++k) {
-        if (k >= cnt) break;
-        double v = acc[k];
-        for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if (l == 0) sh[wid][k] = v;
-    }
-    __syncthreads();
+__device__ __forceinline__ double dot4(const T (&a)[4], const T (&b)[4]) {
+    return double(a[0]) * double(b[0]) + double(a[1]) * double(b[1]) + double(a[2]) * double(b[2]) +
+           double(a[3]) * double(b[3]);
+}
+
+// sum of the per-block values v[0..cnt) over the grid in a fixed order; the last block to arrive
+// writes out[0..cnt) and resets the counter. sh holds the block's per-warp values on entry.
+__device__ void ms_grid_sum(double (*sh)[MS_MAXM], int cnt, double* partials, unsigned* counter, double* out) {
+    __shared__ bool last;
     if (threadIdx.x < cnt) {
         double s = 0;
         for (int q = 0; q < MS_THREADS / 32; ++q) s += sh[q][threadIdx.x];
         partials[(long long)blockIdx.x * MS_MAXM + threadIdx.x] = s;
     }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int k = wid; k < cnt; k += MS_THREADS / 32) {
+        double s = 0;
+        for (int b = l; b < gridDim.x; b += 32) s += __ldcg(partials + (long long)b * MS_MAXM + k);
+        for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+        if (l == 0) out[k] = s;
+    }
+    if (threadIdx.x == 0) *counter = 0;
 }
 
-__global__ void k_mdot_finish(const double* partials, int nb, int cnt, double* out) {
-    const int k = threadIdx.x;
-    if (k >= cnt) return;
-    double s = 0;
-    for (int b = 0; b < nb; ++b) s += partials[(long long)b * MS_MAXM + k];
-    out[k] = s;
-}
-
-// w -= sum_k h[k] V[:, k]
+// out[k] = V[:, k] . w for k < cnt, cnt = (cnt_dev ? *cnt_dev : 0) + cnt_add. Block b stages its
+// rows of w in shared memory and streams the cnt columns over them (two at a time, 16-byte
+// loads); the column stride ld and chunk are multiples of 4.
 template <typename T>
-__global__ void k_gs_update(const T* V, long long ld, int cnt, const double* h, T* w, long long n) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(MS_THREADS) k_mdot(const T* V, long long ld, const int* cnt_dev, int cnt_add,
+                                                     const T* w, long long n, long long chunk, double* partials,
+                                                     unsigned* counter, double* out) {
+    extern __shared__ __align__(16) unsigned char ms_smem[];
+    T* ws = reinterpret_cast<T*>(ms_smem);
+    __shared__ double sh[MS_THREADS / 32][MS_MAXM];
+    const int cnt = min((cnt_dev ? *cnt_dev : 0) + cnt_add, MS_MAXM);
+    const long long lo = blockIdx.x * chunk;
+    const int len = int(max(0LL, min(n, lo + chunk) - lo));
+    const int len4 = len & ~3;
+    for (int i = 4 * threadIdx.x; i < len4; i += 4 * MS_THREADS) {
+        T v[4];
+        ld4(w + lo + i, v);
+        st4(ws + i, v);
+    }
+    for (int i = len4 + threadIdx.x; i < len; i += MS_THREADS) ws[i] = w[lo + i];
+    __syncthreads();
+    const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int k = 0; k < cnt; k += 2) {
+        const bool two = k + 1 < cnt;
+        const T* v0 = V + k * ld + lo;
+        const T* v1 = two ? v0 + ld : v0;
+        double a0 = 0, a1 = 0;
+#pragma unroll 2
+        for (int i = 4 * threadIdx.x; i < len4; i += 4 * MS_THREADS) {
+            T x[4], p[4], q[4];
+            ld4(ws + i, x);
+            ld4(v0 + i, p);
+            ld4(v1 + i, q);
+            a0 += dot4(p, x);
+            a1 += dot4(q, x);
+        }
+        for (int i = len4 + threadIdx.x; i < len; i += MS_THREADS) {
+            a0 += double(v0[i]) * double(ws[i]);
+            a1 += double(v1[i]) * double(ws[i]);
+        }
+        for (int off = 16; off; off >>= 1) {
+            a0 += __shfl_down_sync(0xffffffffu, a0, off);
+            a1 += __shfl_down_sync(0xffffffffu, a1, off);
+        }
+        if (l == 0) {
+            sh[wid][k] = a0;
+            if (two) sh[wid][k + 1] = a1;
+        }
+    }
+    __syncthreads();
+    ms_grid_sum(sh, cnt, partials, counter, out);
+}
+
+// w -= sum_k h[k] V[:, k] (cnt columns, as in k_mdot); with nrm: |w|^2 of the result -> nrm[0]
+template <typename T>
+__global__ void __launch_bounds__(MS_THREADS) k_gs_update(const T* V, long long ld, const int* cnt_dev, int cnt_add,
+                                                          const double* h, T* w, long long n, double* partials,
+                                                          unsigned* counter, double* nrm) {
+    __shared__ T hs[MS_MAXM];
+    __shared__ double sh[MS_THREADS / 32][MS_MAXM];
+    const int cnt = min((cnt_dev ? *cnt_dev : 0) + cnt_add, MS_MAXM);
+    if (threadIdx.x < cnt) hs[threadIdx.x] = T(h[threadIdx.x]);
+    __syncthreads();
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nth = (long long)gridDim.x * blockDim.x;
+    const long long n4 = n & ~3LL;
+    double acc = 0;
+    for (long long i = 4 * tid; i < n4; i += 4 * nth) {
+        T s[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll 4
+        for (int k = 0; k < cnt; ++k) {
+            T a[4];
+            ld4(V + k * ld + i, a);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) s[q] += hs[k] * a[q];
+        }
+        T x[4];
+        ld4(w + i, x);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) x[q] -= s[q];
+        st4(w + i, x);
+        acc += dot4(x, x);
+    }
+    for (long long i = n4 + tid; i < n; i += nth) {
         T s = T(0);
-        for (int k = 0; k < cnt; ++k) s += T(h[k]) * V[k * ld + i];
-        w[i] -= s;
+        for (int k = 0; k < cnt; ++k) s += hs[k] * V[k * ld + i];
+        const T x = w[i] - s;
+        w[i] = x;
+        acc += double(x) * double(x);
+    }
+    if (!nrm) return;
+    for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5][0] = acc;
+    __syncthreads();
+    ms_grid_sum(sh, 1, partials, counter, nrm);
+}
+
+// v = w / sqrt(nrm2[0]) into column (*col + 1) of V and into vnext (the next preconditioner input)
+template <typename T>
+__global__ void __launch_bounds__(MS_THREADS) k_scale_norm(const T* w, const double* nrm2, T* V, long long ld,
+                                                           const int* col, T* vnext, long long n) {
+    const double nr = sqrt(fmax(nrm2[0], 0.0));
+    const double a = nr > 0 ? 1.0 / nr : 0.0;
+    T* v = V + (long long)(col[0] + 1) * ld;
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nth = (long long)gridDim.x * blockDim.x;
+    const long long n4 = n & ~3LL;
+    for (long long i = 4 * tid; i < n4; i += 4 * nth) {
+        T x[4];
+        ld4(w + i, x);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) x[q] = T(a * double(x[q]));
+        st4(v + i, x);
+        st4(vnext + i, x);
+    }
+    for (long long i = n4 + tid; i < n; i += nth) v[i] = vnext[i] = T(a * double(w[i]));
+}
+
+// start of a cycle: beta = sqrt(|t|^2) (hd[65]); V[:, 0] = vnext = t / beta, g = beta e_0, j = 0
+template <typename T>
+__global__ void __launch_bounds__(MS_THREADS) k_cycle_start(const T* t, T* V, T* vnext, long long n, MsKrylov* K,
+                                                            int first) {
+    const double beta = sqrt(fmax(K->hd[65], 0.0));
+    const double a = beta > 0 ? 1.0 / beta : 0.0;
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nth = (long long)gridDim.x * blockDim.x;
+    const long long n4 = n & ~3LL;
+    for (long long i = 4 * tid; i < n4; i += 4 * nth) {
+        T x[4];
+        ld4(t + i, x);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) x[q] = T(a * double(x[q]));
+        st4(V + i, x);
+        st4(vnext + i, x);
+    }
+    for (long long i = n4 + tid; i < n; i += nth) V[i] = vnext[i] = T(a * double(t[i]));
+    if (tid == 0) {
+        for (int i = 0; i <= MS_MAXM; ++i) K->g[i] = 0.0;
+        K->g[0] = beta;
+        K->j = 0;
+        if (first) K->beta0 = beta;
     }
 }
 
-template <typename T>
-__global__ void k_scale_to(const T* w, double a, T* v, long long n) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        v[i] = T(a * double(w[i]));
+__global__ void k_kry_init(MsKrylov* K, double tol, int m, int maxit) {
+    K->tol = tol;
+    K->m = m;
+    K->maxit = maxit;
+    K->its = 0;
+    K->done = 0;
+    K->rel = 1.0;
 }
 
-// t = sum_k y[k] V[:, k]
+// end of an Arnoldi step: Hessenberg column j from the two Gram-Schmidt passes, previous rotations,
+// new rotation, residual estimate |g_{j+1}| / beta0; the loop continues while the cycle has room,
+// the estimate is above tol and the new vector is nonzero
+__global__ void k_givens(MsKrylov* K, cudaGraphConditionalHandle cond) {
+    const int j = K->j;
+    double h[MS_MAXM + 1];
+    for (int i = 0; i <= j; ++i) h[i] = K->hd[i] + K->hd[MS_MAXM + i];
+    const double hn = sqrt(fmax(K->hd[2 * MS_MAXM], 0.0));
+    for (int i = 0; i < j; ++i) {
+        const double a = h[i], b = h[i + 1];
+        h[i] = K->cs[i] * a + K->sn[i] * b;
+        h[i + 1] = -K->sn[i] * a + K->cs[i] * b;
+    }
+    const double den = hypot(h[j], hn);
+    K->cs[j] = den > 0 ? h[j] / den : 1.0;
+    K->sn[j] = den > 0 ? hn / den : 0.0;
+    h[j] = den;
+    K->g[j + 1] = -K->sn[j] * K->g[j];
+    K->g[j] = K->cs[j] * K->g[j];
+    for (int i = 0; i <= j; ++i) K->H[i * MS_MAXM + j] = h[i];
+    K->rel = fabs(K->g[j + 1]) / K->beta0;
+    K->its += 1;
+    K->j = j + 1;
+    K->done = (K->rel <= K->tol || !(hn > 0)) ? 1 : 0;
+    const bool more = !K->done && K->j < K->m && K->its < K->maxit;
+    cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+
+// y = R^{-1} g over the j columns of the cycle
+__global__ void k_trisolve(MsKrylov* K) {
+    const int j = K->j;
+    for (int i = j - 1; i >= 0; --i) {
+        double s = K->g[i];
+        for (int c = i + 1; c < j; ++c) s -= K->H[i * MS_MAXM + c] * K->y[c];
+        const double d = K->H[i * MS_MAXM + i];
+        K->y[i] = d != 0 ? s / d : 0.0;
+    }
+}
+
+// t = sum_{k < *cnt} y[k] V[:, k]
 template <typename T>
-__global__ void k_combine(const T* V, long long ld, int cnt, const double* y, T* t, long long n) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(MS_THREADS) k_combine(const T* V, long long ld, const int* cnt_dev, const double* y,
+                                                        T* t, long long n) {
+    __shared__ double ys[MS_MAXM];
+    const int cnt = min(*cnt_dev, MS_MAXM);
+    if (threadIdx.x < cnt) ys[threadIdx.x] = y[threadIdx.x];
+    __syncthreads();
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nth = (long long)gridDim.x * blockDim.x;
+    const long long n4 = n & ~3LL;
+    for (long long i = 4 * tid; i < n4; i += 4 * nth) {
+        double s[4] = {0, 0, 0, 0};
+#pragma unroll 4
+        for (int k = 0; k < cnt; ++k) {
+            T a[4];
+            ld4(V + k * ld + i, a);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) s[q] += ys[k] * double(a[q]);
+        }
+        T o[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) o[q] = T(s[q]);
+        st4(t + i, o);
+    }
+    for (long long i = n4 + tid; i < n; i += nth) {
         double s = 0;
-        for (int k = 0; k < cnt; ++k) s += y[k] * double(V[k * ld + i]);
+        for (int k = 0; k < cnt; ++k) s += ys[k] * double(V[k * ld + i]);
         t[i] = T(s);
     }
 }
@@ -327,11 +556,14 @@ void Solver::ms_configure(double d12, double d13, double d23, double dt) {
     if (bc != VG_BC_FLUX)
         throw Error(VG_EINVAL, "Maxwell-Stefan needs the no-flux boundary (build the handle with VG_BC_FLUX)");
     if (!(d12 > 0 && d13 > 0 && d23 > 0 && dt > 0)) throw Error(VG_EINVAL, "diffusivities and dt must be positive");
+    ms_destroy_graphs();
     ms_.i12 = 1.0 / d12;
     ms_.i13 = 1.0 / d13;
     ms_.i23 = 1.0 / d23;
     ms_.dt = dt;
     ms_.N = 2LL * nf + 2LL * m.nc;
+    ms_large_ = false;
+    for (const auto& P : pieces_) ms_large_ = ms_large_ || P.n < 3 || P.n > 9;
     const long long Nm = ms_.N;
     ms_.B64.resize(4 * size_t(m.nc));
     ms_.B32.resize(4 * size_t(m.nc));
@@ -343,17 +575,28 @@ void Solver::ms_configure(double d12, double d13, double d23, double dt) {
     ms_.m64.resize(m.nc);
     ms_.m32.resize(m.nc);
     ms_.A32.resize(a_total_);
-    k_d2f<<<MS_BLOCKS, MS_THREADS>>>(d_A0_.data(), ms_.A32.data(), a_total_, 1.0);
-    k_ms_mdt<<<ms_blocks(m.nc), MS_THREADS>>>(d_L_.data(), m.nc, dt, ms_.m64.data(), ms_.m32.data());
+    VG_CUDA(cudaDeviceSynchronize());  // inputs written on other streams
+    k_d2f<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(d_A0_.data(), ms_.A32.data(), a_total_, 1.0);
+    k_ms_mdt<<<ms_blocks(m.nc), MS_THREADS, 0, stream_>>>(d_L_.data(), m.nc, dt, ms_.m64.data(), ms_.m32.data());
     VG_CUDA(cudaGetLastError());
-    ms_.V64.resize(size_t(MS_MAXM) * Nm);
-    ms_.V32.resize(size_t(MS_MAXM) * Nm);
-    for (auto* b : {&ms_.b, &ms_.r, &ms_.y, &ms_.d, &ms_.t64}) b->resize(Nm);
-    for (auto* b : {&ms_.r32, &ms_.d32, &ms_.t32, &ms_.w32}) b->resize(Nm);
+    // Krylov basis with a column stride that keeps every column 16-byte aligned for 4-wide access
+    ms_.ld = (Nm + 63) / 64 * 64;
+    ms_.V64.resize(size_t(MS_MAXM) * ms_.ld);
+    ms_.V32.resize(size_t(MS_MAXM) * ms_.ld);
+    for (auto* b : {&ms_.b, &ms_.r, &ms_.y, &ms_.d, &ms_.t64, &ms_.vn64}) b->resize(Nm);
+    for (auto* b : {&ms_.r32, &ms_.d32, &ms_.t32, &ms_.w32, &ms_.vn32}) b->resize(Nm);
     ms_.w64.resize(Nm);
-    ms_.partials.resize(size_t(MS_BLOCKS) * MS_MAXM);
-    ms_.h.resize(MS_MAXM);
-    VG_CUDA(cudaDeviceSynchronize());
+    // dot-product split: at least one block per SM slot, at most 8192 rows (64 KB of FP64 staging) per block
+    ms_.chunk = std::min<long long>(8192, ((Nm + MS_BLOCKS - 1) / MS_BLOCKS + 3) / 4 * 4);
+    ms_.dblocks = int((Nm + ms_.chunk - 1) / ms_.chunk);
+    ms_.partials.resize(size_t(std::max(ms_.dblocks, MS_BLOCKS)) * MS_MAXM);
+    ms_.counter.resize(1);
+    VG_CUDA(cudaMemsetAsync(ms_.counter.data(), 0, sizeof(unsigned), stream_));
+    ms_.kry.resize((sizeof(MsKrylov) + 7) / 8);
+    VG_CUDA(cudaMemsetAsync(ms_.kry.data(), 0, sizeof(MsKrylov), stream_));
+    VG_CUDA(cudaFuncSetAttribute(k_mdot<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 8));
+    VG_CUDA(cudaFuncSetAttribute(k_mdot<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 4));
+    VG_CUDA(cudaStreamSynchronize(stream_));
     ms_.amg_ready = false;
     ms_.ready = true;
 }
@@ -379,8 +622,9 @@ void Solver::ms_apply(const T* x, T* y) {
     a.nc = m.nc;
     a.nf = nf;
     a.mask = d_mask_.data();
-    VG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * 2 * nf, nullptr));
-    k_ms_apply<T><<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS>>>(a);
+    VG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * 2 * nf, stream_));
+    k_ms_apply<T><<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS, 0, stream_>>>(a);
+    if (ms_large_) k_ms_apply_large<T><<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS, 0, stream_>>>(a);
     VG_CUDA(cudaGetLastError());
     ++n_apply;
     ++n_launch;
@@ -390,16 +634,18 @@ template <typename T>
 void Solver::ms_precond(const T* r, T* z) {
     const T* F = sizeof(T) == 8 ? reinterpret_cast<const T*>(ms_.F64.data()) : reinterpret_cast<const T*>(ms_.F32.data());
     const T* C = sizeof(T) == 8 ? reinterpret_cast<const T*>(ms_.C64.data()) : reinterpret_cast<const T*>(ms_.C32.data());
-    k_ms_pc_apply<T><<<MS_BLOCKS, MS_THREADS>>>(r, z, F, C, nf, m.nc);
+    k_ms_pc_apply<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(r, z, F, C, nf, m.nc);
     VG_CUDA(cudaGetLastError());
     if (ms_.amg_ready)  // pressure blocks: one V-cycle per species (replaces the 2x2 cell blocks)
         for (int s = 0; s < 2; ++s)
-            ms_.amg[s].vcycle(r + 2 * nf + (long long)s * m.nc, z + 2 * nf + (long long)s * m.nc, nullptr);
+            ms_.amg[s].vcycle(r + 2 * nf + (long long)s * m.nc, z + 2 * nf + (long long)s * m.nc, stream_);
 }
 
 // S_s = diag(|E|/dt) + W diag((F_g^{-1})_ss) W^T on the cell graph (k = 0: W = +-1 per local edge,
 // opposite signs across a shared edge), free flux dofs only
 void Solver::ms_build_amg() {
+    ms_destroy_graphs();  // the captured loop holds the previous hierarchy's buffers
+    VG_CUDA(cudaStreamSynchronize(stream_));
     std::vector<double> F = ms_.F64.download(), mdt = ms_.m64.download();
     std::vector<int> mask(nf);
     VG_CUDA(cudaMemcpy(mask.data(), d_mask_.data(), sizeof(int) * nf, cudaMemcpyDeviceToHost));
@@ -442,109 +688,158 @@ void Solver::ms_build_amg() {
         }
         ms_.amg[s].setup(S, nullptr);
     }
+    VG_CUDA(cudaDeviceSynchronize());
     ms_.amg_ready = true;
 }
 
-// dot products of w with columns 0..cnt-1 of V (host result)
+// |x|^2 into device memory
 template <typename T>
-void Solver::ms_dots(const T* V, long long ld, int cnt, const T* w, double* out, int self) {
-    k_mdot<T><<<MS_BLOCKS, MS_THREADS>>>(V, ld, cnt, w, ms_.N, ms_.partials.data(), self);
-    k_mdot_finish<<<1, MS_MAXM>>>(ms_.partials.data(), MS_BLOCKS, cnt + self, ms_.h.data());
+void Solver::ms_norm2(const T* x, double* dst) {
+    k_mdot<T><<<ms_.dblocks, MS_THREADS, ms_.chunk * sizeof(T), stream_>>>(
+        x, 0, nullptr, 1, x, ms_.N, ms_.chunk, ms_.partials.data(), ms_.counter.data(), dst);
     VG_CUDA(cudaGetLastError());
-    VG_CUDA(cudaMemcpy(out, ms_.h.data(), sizeof(double) * (cnt + self), cudaMemcpyDeviceToHost));
 }
 
-// right-preconditioned GMRES(m) on K d = r from d = 0; returns iterations, relative reduction in *rel
+// |x| on the host
 template <typename T>
-int Solver::ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* rel) {
-    const long long Nm = ms_.N;
+double Solver::ms_norm(const T* x) {
+    MsKrylov* K = reinterpret_cast<MsKrylov*>(ms_.kry.data());
+    ms_norm2<T>(x, K->hd + 2 * MS_MAXM + 1);
+    double h = 0;
+    VG_CUDA(cudaMemcpyAsync(&h, K->hd + 2 * MS_MAXM + 1, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    VG_CUDA(cudaStreamSynchronize(stream_));
+    return std::sqrt(std::max(h, 0.0));
+}
+
+void Solver::ms_destroy_graphs() {
+    for (int p = 0; p < 2; ++p) {
+        if (ms_.gexec[p]) cudaGraphExecDestroy(ms_.gexec[p]);
+        if (ms_.graph[p]) cudaGraphDestroy(ms_.graph[p]);
+        ms_.gexec[p] = nullptr;
+        ms_.graph[p] = nullptr;
+    }
+}
+
+// one Arnoldi step on the stream being captured: z = M^{-1} v_j, w = K z, classical Gram-Schmidt
+// applied twice (the second pass restores the orthogonality lost to cancellation), v_{j+1} = w/|w|,
+// then the Givens update that sets the loop condition. The column index j lives on the device.
+template <typename T>
+void Solver::ms_arnoldi_step(cudaGraphConditionalHandle cond) {
+    const long long Nm = ms_.N, ld = ms_.ld;
     T* V = sizeof(T) == 8 ? reinterpret_cast<T*>(ms_.V64.data()) : reinterpret_cast<T*>(ms_.V32.data());
     T* w = sizeof(T) == 8 ? reinterpret_cast<T*>(ms_.w64.data()) : reinterpret_cast<T*>(ms_.w32.data());
     T* t = sizeof(T) == 8 ? reinterpret_cast<T*>(ms_.t64.data()) : reinterpret_cast<T*>(ms_.t32.data());
+    T* vn = sizeof(T) == 8 ? reinterpret_cast<T*>(ms_.vn64.data()) : reinterpret_cast<T*>(ms_.vn32.data());
+    MsKrylov* K = reinterpret_cast<MsKrylov*>(ms_.kry.data());
+    double* part = ms_.partials.data();
+    unsigned* ctr = ms_.counter.data();
+    const size_t smem = ms_.chunk * sizeof(T);
+    ms_precond<T>(vn, t);
+    ms_apply<T>(t, w);
+    for (int pass = 0; pass < 2; ++pass) {
+        double* hd = K->hd + pass * MS_MAXM;
+        k_mdot<T><<<ms_.dblocks, MS_THREADS, smem, stream_>>>(V, ld, &K->j, 1, w, Nm, ms_.chunk, part, ctr, hd);
+        k_gs_update<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(V, ld, &K->j, 1, hd, w, Nm, part, ctr,
+                                                              pass ? K->hd + 2 * MS_MAXM : nullptr);
+    }
+    k_scale_norm<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(w, K->hd + 2 * MS_MAXM, V, ld, &K->j, vn, Nm);
+    k_givens<<<1, 1, 0, stream_>>>(K, cond);
+    VG_CUDA(cudaGetLastError());
+}
+
+// the Arnoldi loop of one cycle as a CUDA graph: a conditional while node around one step
+template <typename T>
+void Solver::ms_build_graph(int p) {
+    VG_CUDA(cudaGraphCreate(&ms_.graph[p], 0));
+    cudaGraphConditionalHandle h;
+    VG_CUDA(cudaGraphConditionalHandleCreate(&h, ms_.graph[p], 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    VG_CUDA(cudaGraphAddNode(&node, ms_.graph[p], nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    VG_CUDA(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const long long napply = n_apply, nlaunch = n_launch;
+    const long long l0 = ms_.amg[0].launches, l1 = ms_.amg[1].launches;
+    try {
+        ms_arnoldi_step<T>(h);
+    } catch (...) {
+        cudaGraph_t dummy;
+        cudaStreamEndCapture(stream_, &dummy);
+        throw;
+    }
+    n_apply = napply;
+    n_launch = nlaunch;
+    ms_.amg[0].launches = l0;
+    ms_.amg[1].launches = l1;
+    VG_CUDA(cudaStreamEndCapture(stream_, &body));
+    VG_CUDA(cudaGraphInstantiate(&ms_.gexec[p], ms_.graph[p], 0));
+}
+
+// right-preconditioned GMRES(m) on K d = r from d = 0; returns iterations, relative reduction in *rel.
+// Per cycle: the captured Arnoldi loop, y = R^{-1} g, d += M^{-1} V y on the device, one host read
+// of the cycle's outcome; on restart t = r - K d and one host read of |t|.
+template <typename T>
+int Solver::ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* rel) {
+    const long long Nm = ms_.N, ld = ms_.ld;
+    T* V = sizeof(T) == 8 ? reinterpret_cast<T*>(ms_.V64.data()) : reinterpret_cast<T*>(ms_.V32.data());
+    T* w = sizeof(T) == 8 ? reinterpret_cast<T*>(ms_.w64.data()) : reinterpret_cast<T*>(ms_.w32.data());
+    T* t = sizeof(T) == 8 ? reinterpret_cast<T*>(ms_.t64.data()) : reinterpret_cast<T*>(ms_.t32.data());
+    T* vn = sizeof(T) == 8 ? reinterpret_cast<T*>(ms_.vn64.data()) : reinterpret_cast<T*>(ms_.vn32.data());
+    MsKrylov* K = reinterpret_cast<MsKrylov*>(ms_.kry.data());
+    const int p = sizeof(T) == 4 ? 1 : 0;
     const int m = std::max(1, std::min(mres, MS_MAXM - 1));
-    VG_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * Nm, nullptr));
+    VG_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * Nm, stream_));
     // residual of the current iterate, kept in t (r initially)
-    VG_CUDA(cudaMemcpyAsync(t, r, sizeof(T) * Nm, cudaMemcpyDeviceToDevice, nullptr));
+    VG_CUDA(cudaMemcpyAsync(t, r, sizeof(T) * Nm, cudaMemcpyDeviceToDevice, stream_));
+    k_kry_init<<<1, 1, 0, stream_>>>(K, tol, m, maxit);
+    ms_norm2<T>(t, K->hd + 2 * MS_MAXM + 1);
     double nr = 0;
-    ms_dots(t, 0, 1, t, &nr, 0);
-    const double beta0 = std::sqrt(nr);
+    VG_CUDA(cudaMemcpyAsync(&nr, K->hd + 2 * MS_MAXM + 1, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    VG_CUDA(cudaStreamSynchronize(stream_));
+    const double beta0 = std::sqrt(std::max(nr, 0.0));
     *rel = 1.0;
     if (!(beta0 > 0)) return 0;
-    int its = 0;
-    std::vector<double> H(size_t(MS_MAXM) * MS_MAXM), cs(MS_MAXM), sn(MS_MAXM), g(MS_MAXM + 1), h(MS_MAXM + 1),
-        h2(MS_MAXM), y(MS_MAXM);
-    double beta = beta0;
-    while (its < maxit) {
-        k_scale_to<T><<<MS_BLOCKS, MS_THREADS>>>(t, 1.0 / beta, V, Nm);
-        std::fill(g.begin(), g.end(), 0.0);
-        g[0] = beta;
-        int j = 0;
-        bool done = false;
-        for (; j < m && its < maxit; ++j) {
-            ++its;
-            ms_precond<T>(V + (long long)j * Nm, t);
-            ms_apply<T>(t, w);
-            // classical Gram-Schmidt applied twice (the second pass restores orthogonality lost to
-            // cancellation); the norm of the result rides on the second projection's pass
-            ms_dots(V, Nm, j + 1, w, h.data(), 0);
-            VG_CUDA(cudaMemcpy(ms_.h.data(), h.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice));
-            k_gs_update<T><<<MS_BLOCKS, MS_THREADS>>>(V, Nm, j + 1, ms_.h.data(), w, Nm);
-            ms_dots(V, Nm, j + 1, w, h2.data(), 0);
-            VG_CUDA(cudaMemcpy(ms_.h.data(), h2.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice));
-            k_gs_update<T><<<MS_BLOCKS, MS_THREADS>>>(V, Nm, j + 1, ms_.h.data(), w, Nm);
-            for (int i = 0; i <= j; ++i) h[i] += h2[i];
-            double nw = 0;
-            ms_dots(w, 0, 1, w, &nw, 0);
-            const double hn = std::sqrt(std::max(nw, 0.0));
-            if (hn > 0) k_scale_to<T><<<MS_BLOCKS, MS_THREADS>>>(w, 1.0 / hn, V + (long long)(j + 1) * Nm, Nm);
-            // Givens rotations of column j
-            for (int i = 0; i < j; ++i) {
-                const double a = h[i], b = h[i + 1];
-                h[i] = cs[i] * a + sn[i] * b;
-                h[i + 1] = -sn[i] * a + cs[i] * b;
-            }
-            const double den = std::hypot(h[j], hn);
-            cs[j] = den > 0 ? h[j] / den : 1.0;
-            sn[j] = den > 0 ? hn / den : 0.0;
-            h[j] = den;
-            g[j + 1] = -sn[j] * g[j];
-            g[j] = cs[j] * g[j];
-            for (int i = 0; i <= j; ++i) H[size_t(i) * MS_MAXM + j] = h[i];
-            *rel = std::fabs(g[j + 1]) / beta0;
-            if (*rel <= tol || !(hn > 0)) {
-                ++j;
-                done = true;
-                break;
-            }
-        }
-        // y = H^{-1} g (upper triangular), d += M^{-1} V y
-        for (int i = j - 1; i >= 0; --i) {
-            double s = g[i];
-            for (int c = i + 1; c < j; ++c) s -= H[size_t(i) * MS_MAXM + c] * y[c];
-            y[i] = H[size_t(i) * MS_MAXM + i] != 0 ? s / H[size_t(i) * MS_MAXM + i] : 0.0;
-        }
-        VG_CUDA(cudaMemcpy(ms_.h.data(), y.data(), sizeof(double) * j, cudaMemcpyHostToDevice));
-        k_combine<T><<<MS_BLOCKS, MS_THREADS>>>(V, Nm, j, ms_.h.data(), w, Nm);
+    if (!ms_.gexec[p]) ms_build_graph<T>(p);
+    struct {
+        double rel;
+        int its, done;
+    } out{};
+    for (int first = 1;; first = 0) {
+        k_cycle_start<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(t, V, vn, Nm, K, first);
+        VG_CUDA(cudaGraphLaunch(ms_.gexec[p], stream_));
+        k_trisolve<<<1, 1, 0, stream_>>>(K);
+        k_combine<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(V, ld, &K->j, K->y, w, Nm);
         ms_precond<T>(w, t);
-        k_axpy_t<T><<<MS_BLOCKS, MS_THREADS>>>(d, t, 1.0, Nm);
+        k_axpy_t<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(d, t, 1.0, Nm);
         VG_CUDA(cudaGetLastError());
-        if (done) break;
+        VG_CUDA(cudaMemcpyAsync(&out.rel, &K->rel, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        VG_CUDA(cudaMemcpyAsync(&out.its, &K->its, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        VG_CUDA(cudaMemcpyAsync(&out.done, &K->done, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        VG_CUDA(cudaStreamSynchronize(stream_));
+        *rel = out.rel;
+        if (out.done || out.its >= maxit) break;
         // restart: t = r - K d
         ms_apply<T>(d, w);
         if constexpr (sizeof(T) == 8) {
-            k_sub<<<MS_BLOCKS, MS_THREADS>>>(reinterpret_cast<const double*>(r), reinterpret_cast<const double*>(w),
-                                            reinterpret_cast<double*>(t), Nm);
+            k_sub<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(reinterpret_cast<const double*>(r),
+                                                         reinterpret_cast<const double*>(w),
+                                                         reinterpret_cast<double*>(t), Nm);
         } else {
-            VG_CUDA(cudaMemcpyAsync(t, r, sizeof(T) * Nm, cudaMemcpyDeviceToDevice, nullptr));
-            k_axpy_t<T><<<MS_BLOCKS, MS_THREADS>>>(t, w, -1.0, Nm);
+            VG_CUDA(cudaMemcpyAsync(t, r, sizeof(T) * Nm, cudaMemcpyDeviceToDevice, stream_));
+            k_axpy_t<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(t, w, -1.0, Nm);
         }
-        double nt = 0;
-        ms_dots(t, 0, 1, t, &nt, 0);
-        beta = std::sqrt(nt);
+        ms_norm2<T>(t, K->hd + 2 * MS_MAXM + 1);
+        VG_CUDA(cudaMemcpyAsync(&nr, K->hd + 2 * MS_MAXM + 1, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        VG_CUDA(cudaStreamSynchronize(stream_));
+        const double beta = std::sqrt(std::max(nr, 0.0));
         *rel = beta / beta0;
         if (*rel <= tol || !(beta > 0)) break;
     }
-    return its;
+    return out.its;
 }
 
 __global__ void k_cell_areas(const double* L, int nc, int q, double* out) {
@@ -561,7 +856,7 @@ void Solver::cell_areas(double* out) {
 
 void Solver::ms_coefficients(const double* state) {
     if (!ms_.ready) throw Error(VG_ESTATE, "vg_ms_configure must run first");
-    k_ms_coeff<<<ms_blocks(m.nc), MS_THREADS>>>(state, 2 * nf, m.nc, ms_.i12, ms_.i13, ms_.i23, ms_.B64.data(),
+    k_ms_coeff<<<ms_blocks(m.nc), MS_THREADS, 0, stream_>>>(state, 2 * nf, m.nc, ms_.i12, ms_.i13, ms_.i23, ms_.B64.data(),
                                                ms_.B32.data());
     VG_CUDA(cudaGetLastError());
 }
@@ -572,39 +867,37 @@ void Solver::ms_step(const double* old_state, double* new_state, const vg_solve_
         throw Error(VG_EINVAL, "invalid solve options");
     info = vg_solve_info{};
     const long long Nm = ms_.N;
-    VG_CUDA(cudaDeviceSynchronize());
-    VG_CUDA(cudaEventRecord(ev0_, nullptr));
+    VG_CUDA(cudaDeviceSynchronize());  // the states may come from any stream
+    VG_CUDA(cudaEventRecord(ev0_, stream_));
     // coefficients and preconditioner at x^n
     ms_coefficients(old_state);
-    ms_.D.zero();
-    k_ms_pc_flux<<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS>>>(
+    VG_CUDA(cudaMemsetAsync(ms_.D.data(), 0, sizeof(double) * ms_.D.size(), stream_));
+    k_ms_pc_flux<<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS, 0, stream_>>>(
         d_A0_.data(), d_map_.data(), d_pieces_.data(), int(pieces_.size()), d_slot_cell_.data(), ms_.B64.data(),
         d_mask_.data(), ms_.D.data());
-    k_ms_pc_flux_inv<<<MS_BLOCKS, MS_THREADS>>>(ms_.D.data(), d_mask_.data(), nf, ms_.F64.data(), ms_.F32.data());
-    k_ms_pc_cell<<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS>>>(
+    k_ms_pc_flux_inv<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(ms_.D.data(), d_mask_.data(), nf, ms_.F64.data(), ms_.F32.data());
+    k_ms_pc_cell<<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS, 0, stream_>>>(
         d_map_.data(), d_pieces_.data(), int(pieces_.size()), d_slot_cell_.data(), d_mask_.data(), ms_.F64.data(),
         ms_.m64.data(), ms_.C64.data(), ms_.C32.data());
     if (!ms_.amg_ready) {
-        VG_CUDA(cudaDeviceSynchronize());
+        VG_CUDA(cudaStreamSynchronize(stream_));
         try {
             ms_build_amg();
         } catch (const Error&) {
             ms_.amg_ready = false;  // the 2x2 cell blocks stay in use
         }
     }
-    k_ms_rhs<<<MS_BLOCKS, MS_THREADS>>>(old_state, ms_.m64.data(), nf, m.nc, ms_.b.data());
+    k_ms_rhs<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(old_state, ms_.m64.data(), nf, m.nc, ms_.b.data());
     VG_CUDA(cudaGetLastError());
     // initial guess: the old state
     if (new_state != old_state)
-        VG_CUDA(cudaMemcpyAsync(new_state, old_state, sizeof(double) * Nm, cudaMemcpyDeviceToDevice, nullptr));
+        VG_CUDA(cudaMemcpyAsync(new_state, old_state, sizeof(double) * Nm, cudaMemcpyDeviceToDevice, stream_));
     auto true_residual = [&](double* nb_out) {
         ms_apply<double>(new_state, ms_.y.data());
-        k_sub<<<MS_BLOCKS, MS_THREADS>>>(ms_.b.data(), ms_.y.data(), ms_.r.data(), Nm);
-        double nr = 0, nb = 0;
-        ms_dots(ms_.r.data(), 0, 1, ms_.r.data(), &nr, 0);
-        ms_dots(ms_.b.data(), 0, 1, ms_.b.data(), &nb, 0);
-        if (nb_out) *nb_out = std::sqrt(nb);
-        return std::sqrt(nr) / (nb > 0 ? std::sqrt(nb) : 1.0);
+        k_sub<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(ms_.b.data(), ms_.y.data(), ms_.r.data(), Nm);
+        const double nr = ms_norm<double>(ms_.r.data()), nbv = ms_norm<double>(ms_.b.data());
+        if (nb_out) *nb_out = nbv;
+        return nr / (nbv > 0 ? nbv : 1.0);
     };
     double nb = 0;
     double rel = true_residual(&nb);
@@ -616,20 +909,20 @@ void Solver::ms_step(const double* old_state, double* new_state, const vg_solve_
             const double rn = rel * nb;
             total += ms_gmres<double>(ms_.r.data(), ms_.d.data(), std::min(0.5, 0.5 * o.tol * nb / rn), o.maxit - total,
                                       mres, &r_in);
-            k_axpy_t<double><<<MS_BLOCKS, MS_THREADS>>>(new_state, ms_.d.data(), 1.0, Nm);
+            k_axpy_t<double><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(new_state, ms_.d.data(), 1.0, Nm);
             rel = true_residual(nullptr);
         }
     } else {
         for (outer = 0; outer < o.max_outer && rel > o.tol && total < o.maxit; ++outer) {
             const double rn = rel * nb;
-            k_d2f<<<MS_BLOCKS, MS_THREADS>>>(ms_.r.data(), ms_.r32.data(), Nm, 1.0 / rn);
+            k_d2f<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(ms_.r.data(), ms_.r32.data(), Nm, 1.0 / rn);
             double r_in = 0;
             total += ms_gmres<float>(ms_.r32.data(), ms_.d32.data(), o.inner_tol, o.maxit - total, mres, &r_in);
-            k_addf<<<MS_BLOCKS, MS_THREADS>>>(new_state, ms_.d32.data(), rn, Nm);
+            k_addf<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(new_state, ms_.d32.data(), rn, Nm);
             rel = true_residual(nullptr);
         }
     }
-    VG_CUDA(cudaEventRecord(ev1_, nullptr));
+    VG_CUDA(cudaEventRecord(ev1_, stream_));
     VG_CUDA(cudaEventSynchronize(ev1_));
     float ms = 0;
     VG_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));

@@ -284,6 +284,7 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
 
 Solver::~Solver() {
     destroy_graphs();
+    ms_destroy_graphs();
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (ev_in_) cudaEventDestroy(ev_in_);

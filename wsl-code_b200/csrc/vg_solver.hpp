@@ -111,20 +111,33 @@ private:
     template <typename T>
     void ms_precond(const T* r, T* z);
     template <typename T>
-    void ms_dots(const T* V, long long ld, int cnt, const T* w, double* out, int self);
+    void ms_norm2(const T* x, double* dst);
+    template <typename T>
+    double ms_norm(const T* x);
+    template <typename T>
+    void ms_arnoldi_step(cudaGraphConditionalHandle cond);
+    template <typename T>
+    void ms_build_graph(int p);
+    void ms_destroy_graphs();
     template <typename T>
     int ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* rel);
     struct MsState {
         bool ready = false;
         double i12 = 0, i13 = 0, i23 = 0, dt = 0;
         long long N = 0;
-        DevBuf<double> B64, F64, C64, D, m64, V64, b, r, y, d, t64, w64, partials, h;
-        DevBuf<float> B32, F32, C32, m32, A32, V32, r32, d32, t32, w32;
+        DevBuf<double> B64, F64, C64, D, m64, V64, b, r, y, d, t64, w64, vn64, partials, kry;
+        DevBuf<float> B32, F32, C32, m32, A32, V32, r32, d32, t32, w32, vn32;
+        DevBuf<unsigned int> counter;
+        long long ld = 0, chunk = 0;  // Krylov basis column stride; rows per dot-product block
+        int dblocks = 0;
+        cudaGraph_t graph[2] = {nullptr, nullptr};  // captured Arnoldi loops (FP64, FP32)
+        cudaGraphExec_t gexec[2] = {nullptr, nullptr};
         // per-species multigrid of the pressure Schur block, built from the first state stepped
         // after vg_ms_configure and kept for the following steps
         Amg amg[2];
         bool amg_ready = false;
     } ms_;
+    bool ms_large_ = false;  // pieces of polygons outside 3..9 edges (second apply kernel)
     void ms_build_amg();
     void assembled_pattern();
     std::vector<long long> csr_ptr_;  // assembled pattern (host, built on first request)
