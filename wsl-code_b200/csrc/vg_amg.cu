@@ -15,6 +15,7 @@
 #include <numeric>
 
 #include "vg_amg.hpp"
+#include "vg_pipe.cuh"
 
 namespace vg {
 
@@ -251,6 +252,8 @@ std::vector<double> dense_of(const HostCsr& A) {
 // device kernels (SELL-32, one thread per row)
 // ---------------------------------------------------------------------------------------------
 constexpr int TPB = 256;
+constexpr int CSR_CAP = 2048;  // entries staged per CSR row block
+constexpr int CSR_RPT = 4;     // rows per thread of a CSR row block (at most CSR_RPT * TPB rows)
 
 // one row of a SELL-32 matrix: sum_k val_k xv(col_k), entries loaded four at a time before their
 // gathers (independent loads in flight), fixed summation order
@@ -293,11 +296,16 @@ __global__ void __launch_bounds__(TPB) k_jacobi0(int n, const T* dinv, T omega, 
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_jacobi0_residual(DevSell<T> A, const T* dinv, T omega, const T* b, T* t,
                                                           T* r) {
+    pdl_trigger();
+    pdl_wait();
     int i = blockIdx.x * TPB + threadIdx.x;
     if (i >= A.n) return;
-    const T acc = sell_dot(A, i, [&](int c) { return omega * dinv[c] * b[c]; });
-    t[i] = omega * dinv[i] * b[i];
-    r[i] = b[i] - acc;
+    // vectors written by earlier kernels of the cycle are read with plain loads after the wait
+    // (never ld.global.nc, which the compiler may move above it)
+    const T acc = sell_dot(A, i, [&](int c) { return omega * __ldg(dinv + c) * b[c]; });
+    const T bi = b[i];
+    t[i] = omega * dinv[i] * bi;
+    r[i] = bi - acc;
 }
 
 template <typename T>
@@ -320,72 +328,206 @@ __global__ void __launch_bounds__(TPB) k_prolong_add(DevSell<T> P, const T* xc, 
 
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_smooth(DevSell<T> A, const T* dinv, T omega, const T* b, const T* x, T* xo) {
+    pdl_trigger();
+    pdl_wait();
     int i = blockIdx.x * TPB + threadIdx.x;
-    if (i < A.n) xo[i] = x[i] + omega * dinv[i] * (b[i] - sell_row(A, i, x));
+    if (i < A.n)
+        xo[i] = x[i] + omega * dinv[i] * (b[i] - sell_dot(A, i, [&](int c) { return x[c]; }));
 }
 
-// ---- CSR, one group of G lanes per row
-template <int G, typename T>
-__device__ __forceinline__ T csr_row(const DevCsr<T>& M, int r, const T* x, int gl) {
-    T acc = T(0);
-    const int lo = __ldg(M.ptr + r), hi = __ldg(M.ptr + r + 1);
-    for (int j = lo + gl; j < hi; j += G) acc += __ldg(M.val + j) * x[__ldg(M.col + j)];
-#pragma unroll
-    for (int off = G / 2; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off, G);
-    return acc;  // valid in lane gl == 0 of the group
+// ---- CSR in row blocks (the CSR-stream scheme of Greathouse and Daga, SC 2014, with the entries
+// staged by bulk copies): row block b covers rows [rb[b].x, rb[b + 1].x) (at most CSR_RPT * TPB)
+// and entries [rb[b].y, rb[b + 1].y) (at most CSR_CAP unless one row alone is longer). A CTA walks
+// row blocks b = blockIdx.x, + gridDim.x, ... through a two-stage ring: the column indices and
+// values of the next row block are copied into shared memory (cp.async.bulk on an mbarrier, 16-byte
+// aligned supersets of the ranges) while the current one gathers x and sums; one thread per row
+// sums its products in order, so the result does not depend on the launch shape. Vectors written
+// by earlier kernels of the cycle are read with plain loads after the programmatic-launch wait
+// (never ld.global.nc, which the compiler may move above it); the matrix may be read before it.
+// op: 0 y = M x; 1 y += M x (prolongation); 2 smoothing y = x + omega dinv (b - M x);
+//     3 Jacobi from zero with its residual: y = omega dinv b, r = b - M y
+template <typename T>
+struct CsrSmem {
+    static constexpr int col_bytes = (CSR_CAP + 8) * 4;
+    static constexpr int val_bytes = (CSR_CAP + 8) * int(sizeof(T));
+    static constexpr int stage_bytes = col_bytes + val_bytes;
+    static constexpr int prod_off = 2 * stage_bytes;
+    static constexpr int total = prod_off + CSR_CAP * int(sizeof(T));
+    static_assert(col_bytes % 16 == 0 && val_bytes % 16 == 0, "16-byte stage layout");
+};
+
+template <int OP, typename T>
+__device__ __forceinline__ T csr_x(int c, const T* dinv, T omega, const T* b, const T* x) {
+    if (OP == 3) return omega * __ldg(dinv + c) * b[c];
+    return x[c];
 }
 
-template <int G, typename T>
-__device__ __forceinline__ T csr_row_jac(const DevCsr<T>& M, int r, const T* dinv, T omega, const T* b, int gl) {
-    T acc = T(0);
-    const int lo = __ldg(M.ptr + r), hi = __ldg(M.ptr + r + 1);
-    for (int j = lo + gl; j < hi; j += G) {
-        int c = __ldg(M.col + j);
-        acc += __ldg(M.val + j) * (omega * dinv[c] * b[c]);
+template <int OP, typename T>
+__global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega, const T* b, const T* x, T* y, T* r) {
+    using L = CsrSmem<T>;
+    constexpr int J = CSR_CAP / TPB;
+    constexpr int VA = 16 / int(sizeof(T));  // values per 16 bytes
+    extern __shared__ __align__(128) unsigned char sm[];
+    __shared__ __align__(8) unsigned long long full[2];
+    __shared__ T red[TPB / 32];
+    T* prod = reinterpret_cast<T*>(sm + L::prod_off);
+    const int t = threadIdx.x, G = gridDim.x, nblk = M.nblk;
+    // copy row block blk into stage s (thread 0); empty and long-row blocks are not staged
+    auto issue = [&](int blk, int s) {
+        const int2 a = __ldg(M.rb + blk), z = __ldg(M.rb + blk + 1);
+        const int ne = z.y - a.y;
+        if (ne <= 0 || ne > CSR_CAP) return;
+        const int c0 = a.y & ~3, c1 = (z.y + 3) & ~3, v0 = a.y & ~(VA - 1), v1 = (z.y + VA - 1) & ~(VA - 1);
+        unsigned char* st = sm + s * L::stage_bytes;
+        mbar_expect_tx(&full[s], unsigned((c1 - c0) * 4 + (v1 - v0) * int(sizeof(T))));
+        bulk_g2s(st, M.col + c0, unsigned((c1 - c0) * 4), &full[s]);
+        bulk_g2s(st + L::col_bytes, M.val + v0, unsigned((v1 - v0) * int(sizeof(T))), &full[s]);
+    };
+    pdl_trigger();
+    if (t == 0) {  // the matrix does not depend on earlier kernels: its first two row blocks are copied before the wait
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+        if (blockIdx.x < nblk) issue(blockIdx.x, 0);
+        if (blockIdx.x + G < nblk) issue(blockIdx.x + G, 1);
     }
+    __syncthreads();
+    pdl_wait();
+    unsigned par0 = 0u, par1 = 0u;  // phase parity of each stage's barrier
+    for (int i = 0, blk = blockIdx.x; blk < nblk; ++i, blk += G) {
+        const int s = i & 1;
+        const int2 a = __ldg(M.rb + blk), z = __ldg(M.rb + blk + 1);
+        const int ne = z.y - a.y;
+        const bool staged = ne > 0 && ne <= CSR_CAP;
+        int lo[CSR_RPT], hi[CSR_RPT];
 #pragma unroll
-    for (int off = G / 2; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off, G);
-    return acc;
+        for (int q = 0; q < CSR_RPT; ++q) {
+            const int row = a.x + t + q * TPB;
+            lo[q] = hi[q] = 0;
+            if (row < z.x) {
+                lo[q] = __ldg(M.ptr + row) - a.y;
+                hi[q] = __ldg(M.ptr + row + 1) - a.y;
+            }
+        }
+        int c[J];
+        T v[J];
+        if (staged) {
+            const bool ok = mbar_wait(&full[s], s ? par1 : par0, nullptr);
+            if (s)
+                par1 ^= 1u;
+            else
+                par0 ^= 1u;
+            if (__syncthreads_or(!ok)) {  // a copy that never landed: flag it and stop (never in a correct run)
+                if (t == 0) {
+                    atomicExch(M.err, 1);
+                    if (blk + G < nblk) mbar_wait(&full[s ^ 1], s ? par0 : par1, nullptr);
+                }
+                return;
+            }
+            const int* scol = reinterpret_cast<const int*>(sm + s * L::stage_bytes) + (a.y & 3);
+            const T* sval = reinterpret_cast<const T*>(sm + s * L::stage_bytes + L::col_bytes) + (a.y & (VA - 1));
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                const int k = t + j * TPB;
+                c[j] = k < ne ? scol[k] : 0;
+                v[j] = k < ne ? sval[k] : T(0);
+            }
+        }
+        __syncthreads();  // stage s consumed: refill it with the row block two steps ahead
+        if (t == 0 && blk + 2 * G < nblk) {
+            fence_proxy_async_smem();
+            issue(blk + 2 * G, s);
+        }
+        T acc[CSR_RPT];
+#pragma unroll
+        for (int q = 0; q < CSR_RPT; ++q) acc[q] = T(0);
+        if (staged) {
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                const int k = t + j * TPB;
+                if (k < ne) prod[k] = v[j] * csr_x<OP>(c[j], dinv, omega, b, x);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < CSR_RPT; ++q)
+                for (int k = lo[q]; k < hi[q]; ++k) acc[q] += prod[k];
+            __syncthreads();  // prod is rewritten by the next row block
+        } else if (ne > CSR_CAP) {  // one long row: strided partial sums, fixed-order block reduction
+            T part = T(0);
+            for (int k = t; k < ne; k += TPB)
+                part += __ldg(M.val + a.y + k) * csr_x<OP>(__ldg(M.col + a.y + k), dinv, omega, b, x);
+            for (int off = 16; off; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+            if ((t & 31) == 0) red[t >> 5] = part;
+            __syncthreads();
+            if (t == 0) {
+                T sum = T(0);
+                for (int w = 0; w < TPB / 32; ++w) sum += red[w];
+                acc[0] = sum;
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int q = 0; q < CSR_RPT; ++q) {
+            const int row = a.x + t + q * TPB;
+            if (row >= z.x) continue;
+            if (OP == 0)
+                y[row] = acc[q];
+            else if (OP == 1)
+                y[row] += acc[q];
+            else if (OP == 2)
+                y[row] = x[row] + omega * dinv[row] * (b[row] - acc[q]);
+            else {
+                const T br = b[row];
+                y[row] = omega * dinv[row] * br;
+                r[row] = br - acc[q];
+            }
+        }
+    }
 }
 
-// op: 0 y = M x; 1 x += M xc (prolong); 2 smooth xo = x + omega dinv (b - M x); 3 jacobi0 + residual
-template <int G, typename T>
-__global__ void __launch_bounds__(TPB) k_csr(int op, DevCsr<T> M, const T* dinv, T omega, const T* b, const T* x,
-                                             T* y, T* r) {
-    int t = blockIdx.x * TPB + threadIdx.x;
-    int row = t / G, gl = t % G;
-    bool ok = row < M.n;
-    int rr = ok ? row : M.n - 1;  // whole groups stay converged for the shuffles
-    T v;
-    if (op == 3)
-        v = csr_row_jac<G>(M, rr, dinv, omega, b, ok ? gl : G);
-    else
-        v = csr_row<G>(M, rr, x, ok ? gl : G);
-    if (!ok || gl != 0) return;
-    if (op == 0)
-        y[row] = v;
-    else if (op == 1)
-        y[row] += v;
-    else if (op == 2)
-        y[row] = x[row] + omega * dinv[row] * (b[row] - v);
-    else {
-        y[row] = omega * dinv[row] * b[row];
-        r[row] = b[row] - v;
-    }
+// CTAs resident per SM of the CSR kernels (shared memory bound), set once
+int g_csr_ctas[2] = {0, 0};  // FP32, FP64
+int g_sm_count = 0;
+
+template <int OP, typename T>
+void prepare_csr_op() {
+    VG_CUDA(cudaFuncSetAttribute(k_csr<OP, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, CsrSmem<T>::total));
+    // the whole unified L1/shared array as shared memory: the occupancy the grid is sized for
+    VG_CUDA(cudaFuncSetAttribute(k_csr<OP, T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 int(cudaSharedmemCarveoutMaxShared)));
+}
+
+void prepare_csr_kernels() {
+    if (g_sm_count) return;
+    prepare_csr_op<0, float>();
+    prepare_csr_op<1, float>();
+    prepare_csr_op<2, float>();
+    prepare_csr_op<3, float>();
+    prepare_csr_op<0, double>();
+    prepare_csr_op<1, double>();
+    prepare_csr_op<2, double>();
+    prepare_csr_op<3, double>();
+    int dev = 0, n32 = 0, n64 = 0, sms = 0;
+    VG_CUDA(cudaGetDevice(&dev));
+    VG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n32, k_csr<3, float>, TPB, CsrSmem<float>::total));
+    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n64, k_csr<3, double>, TPB, CsrSmem<double>::total));
+    g_csr_ctas[0] = std::max(1, n32);
+    g_csr_ctas[1] = std::max(1, n64);
+    g_sm_count = std::max(1, sms);
 }
 
 template <typename T>
 void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, const T* x, T* y, T* r,
                 cudaStream_t s) {
-    if (M.n <= 0) return;
-    long long threads = (long long)M.n * M.group;
-    int blocks = int((threads + TPB - 1) / TPB);
-    switch (M.group) {
-    case 2: k_csr<2, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
-    case 4: k_csr<4, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
-    case 8: k_csr<8, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
-    case 16: k_csr<16, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
-    default: k_csr<32, T><<<blocks, TPB, 0, s>>>(op, M, dinv, omega, b, x, y, r); break;
+    if (M.n <= 0 || M.nblk <= 0) return;
+    const int grid = std::min(M.nblk, g_sm_count * g_csr_ctas[sizeof(T) == 8 ? 1 : 0]);
+    const int sb = CsrSmem<T>::total;
+    switch (op) {
+    case 0: launch_pdl(k_csr<0, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
+    case 1: launch_pdl(k_csr<1, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
+    case 2: launch_pdl(k_csr<2, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
+    default: launch_pdl(k_csr<3, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
     }
 }
 
@@ -394,16 +536,25 @@ void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, 
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_dense(int n, const T* Ainv, const T* b, T* z) {
     __shared__ T sh[TPB / 32];
+    pdl_trigger();
     const int row = blockIdx.x, t = threadIdx.x;
     const T* a = Ainv + (long long)row * n;
-    T acc0 = T(0), acc1 = T(0);
-    int j = t;
-    for (; j + TPB < n; j += 2 * TPB) {
-        T a0 = __ldcs(a + j), a1 = __ldcs(a + j + TPB);
-        acc0 += a0 * __ldg(b + j);
-        acc1 += a1 * __ldg(b + j + TPB);
+    // the row of the inverse does not depend on earlier kernels: load it before the wait
+    constexpr int PRE = (DENSE_MAX + TPB - 1) / TPB;
+    T av[PRE];
+#pragma unroll
+    for (int q = 0; q < PRE; ++q) {
+        const int j = t + q * TPB;
+        av[q] = j < n ? __ldcs(a + j) : T(0);
     }
-    if (j < n) acc0 += __ldcs(a + j) * __ldg(b + j);
+    pdl_wait();
+    T acc0 = T(0), acc1 = T(0);
+#pragma unroll
+    for (int q = 0; q < PRE; q += 2) {
+        const int j = t + q * TPB;
+        if (j < n) acc0 += av[q] * b[j];
+        if (q + 1 < PRE && j + TPB < n) acc1 += av[q + 1] * b[j + TPB];
+    }
     T acc = acc0 + acc1;
     for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
     if ((t & 31) == 0) sh[t >> 5] = acc;
@@ -669,20 +820,33 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
             L.dinv[i] = d != 0.0 ? 1.0 / d : 0.0;
         }
         // storage: SELL-32 (one thread per row) only for the regular fine-level operator; every other
-        // matrix (rectangular P and R, the denser coarse operators) as CSR with a group of lanes per
-        // row sized to about three entries per lane (a power of two in 2..32)
+        // matrix (rectangular P and R, the denser coarse operators) as CSR in row blocks (k_csr)
         auto to_sell = [&](const HostCsr& M, Sell& S, bool sell_ok) {
             S.n = M.n;
             double avg = M.n ? double(M.col.size()) / M.n : 0.0;
             if (!(sell_ok && avg <= 10.0)) {
                 S.csr = true;
-                int g = 2;
-                while (g < 32 && 3.0 * g * 1.41421356 < avg) g *= 2;
-                S.group = g;
                 S.cptr = M.ptr;
                 S.ccol = M.col;
                 S.cval = M.val;
                 S.nslices = 0;
+                // row blocks: at most CSR_RPT * TPB rows and about nnz / (4 blocks per SM) entries,
+                // between 256 and CSR_CAP (a longer single row is a block of its own)
+                const long long nnz = (long long)M.col.size();
+                const int cap = int(std::min<long long>(CSR_CAP, std::max<long long>(256, (nnz + 591) / 592)));
+                S.rb.assign({0, 0});
+                for (int r = 0; r < M.n;) {
+                    const int start = r;
+                    long long nn = 0;
+                    while (r < M.n && r - start < CSR_RPT * TPB) {
+                        const int len = M.ptr[r + 1] - M.ptr[r];
+                        if (r > start && nn + len > cap) break;
+                        nn += len;
+                        ++r;
+                    }
+                    S.rb.push_back(r);
+                    S.rb.push_back(M.ptr[r]);
+                }
                 return;
             }
             S.nslices = (M.n + 31) / 32;
@@ -771,7 +935,7 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
         pt.mark("multigrid level (host)");
     }
     // coarsest level: dense inverse (bounded size; otherwise the caller keeps its diagonal preconditioner)
-    if (A.n > 4096) {
+    if (A.n > DENSE_MAX) {
         levels_.clear();
         throw Error(VG_EINVAL, "multigrid coarsening stalled at " + std::to_string(A.n) + " rows");
     }
@@ -804,28 +968,38 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
         up(L.A, L.dA_soff, L.dA_w, L.dA_col, L.dA_v64, L.dA_v32);
         up(L.P, L.dP_soff, L.dP_w, L.dP_col, L.dP_v64, L.dP_v32);
         up(L.R, L.dR_soff, L.dR_w, L.dR_col, L.dR_v64, L.dR_v32);
-        auto upc = [](const Sell& S, DevBuf<int>& p, DevBuf<int>& c, DevBuf<double>& v64, DevBuf<float>& v32) {
+        auto upc = [](const Sell& S, DevBuf<int>& p, DevBuf<int>& c, DevBuf<double>& v64, DevBuf<float>& v32,
+                      DevBuf<int>& rb) {
             if (S.n == 0 || !S.csr) return;
+            rb.upload(S.rb);
             p.upload(S.cptr);
-            c.upload(S.ccol);
-            v64.upload(S.cval);
-            std::vector<float> f(S.cval.begin(), S.cval.end());
+            // column and value arrays padded by 4 entries: k_csr copies 16-byte aligned supersets
+            std::vector<int> cc(S.ccol);
+            cc.resize(cc.size() + 4, 0);
+            c.upload(cc);
+            std::vector<double> vv(S.cval);
+            vv.resize(vv.size() + 4, 0.0);
+            v64.upload(vv);
+            std::vector<float> f(vv.begin(), vv.end());
             v32.upload(f);
         };
-        upc(L.A, L.cA_ptr, L.cA_col, L.cA_v64, L.cA_v32);
+        upc(L.A, L.cA_ptr, L.cA_col, L.cA_v64, L.cA_v32, L.cA_rb);
         L.dpa_ptr.upload(L.pa_ptr);
         L.dpa_col.upload(L.pa_col);
         if (!L.agg.empty()) L.dagg.upload(L.agg);
         if (!L.r2p.empty()) L.dr2p.upload(L.r2p);
         if (!L.sellpos.empty()) L.dsellpos.upload(L.sellpos);
-        upc(L.P, L.cP_ptr, L.cP_col, L.cP_v64, L.cP_v32);
-        upc(L.R, L.cR_ptr, L.cR_col, L.cR_v64, L.cR_v32);
+        upc(L.P, L.cP_ptr, L.cP_col, L.cP_v64, L.cP_v32, L.cP_rb);
+        upc(L.R, L.cR_ptr, L.cR_col, L.cR_v64, L.cR_v32, L.cR_rb);
         L.dinv64.upload(L.dinv);
         std::vector<float> f(L.dinv.begin(), L.dinv.end());
         L.dinv32.upload(f);
         for (auto* b : {&L.x64, &L.b64, &L.r64, &L.t64}) b->resize(L.n);
         for (auto* b : {&L.x32, &L.b32, &L.r32, &L.t32}) b->resize(L.n);
     }
+    err_.resize(1);
+    err_.zero();
+    prepare_csr_kernels();
     pt.mark("multigrid uploads");
 }
 
@@ -853,7 +1027,9 @@ DevCsr<T> Amg::cview(const Level& L, int which) const {
     DevCsr<T> v;
     const Sell& S = which == 0 ? L.A : which == 1 ? L.P : L.R;
     v.n = S.n;
-    v.group = S.group;
+    v.nblk = S.csr ? int(S.rb.size() / 2) - 1 : 0;
+    v.err = const_cast<int*>(err_.data());
+    v.rb = reinterpret_cast<const int2*>((which == 0 ? L.cA_rb : which == 1 ? L.cP_rb : L.cR_rb).data());
     v.ptr = (which == 0 ? L.cA_ptr : which == 1 ? L.cP_ptr : L.cR_ptr).data();
     v.col = (which == 0 ? L.cA_col : which == 1 ? L.cP_col : L.cR_col).data();
     if constexpr (sizeof(T) == 8)
@@ -876,7 +1052,7 @@ void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     if (l == int(levels_.size()) - 1) {
         const T* inv = sizeof(T) == 8 ? reinterpret_cast<const T*>(dinvc64_.data())
                                       : reinterpret_cast<const T*>(dinvc32_.data());
-        k_dense<T><<<ncoarse_, TPB, 0, s>>>(ncoarse_, inv, b, z);
+        launch_pdl(k_dense<T>, ncoarse_, TPB, 0, s, ncoarse_, inv, b, z);
         ++launches;
         return;
     }
@@ -890,7 +1066,7 @@ void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     if (L.A.csr)
         launch_csr<T>(3, cview<T>(L, 0), dinv, om, b, nullptr, t, r, s);
     else
-        k_jacobi0_residual<T><<<blocks(L.n), TPB, 0, s>>>(view<T>(L, 0), dinv, om, b, t, r);
+        launch_pdl(k_jacobi0_residual<T>, blocks(L.n), TPB, 0, s, view<T>(L, 0), dinv, om, b, t, r);
     // restriction
     if (L.R.csr)
         launch_csr<T>(0, cview<T>(L, 2), nullptr, T(0), nullptr, r, bc, nullptr, s);
@@ -907,8 +1083,16 @@ void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     if (L.A.csr)
         launch_csr<T>(2, cview<T>(L, 0), dinv, om, b, t, z, nullptr, s);
     else
-        k_smooth<T><<<blocks(L.n), TPB, 0, s>>>(view<T>(L, 0), dinv, om, b, t, z);
+        launch_pdl(k_smooth<T>, blocks(L.n), TPB, 0, s, view<T>(L, 0), dinv, om, b, t, z);
     launches += 2;
+}
+
+bool Amg::failed() {
+    if (err_.size() == 0) return false;
+    int e = 0;
+    VG_CUDA(cudaMemcpy(&e, err_.data(), sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) err_.zero();
+    return e != 0;
 }
 
 void Amg::vcycle(const double* b, double* z, cudaStream_t s) {

@@ -30,11 +30,13 @@ struct DevSell {
     const T* val = nullptr;
 };
 
-// CSR for matrices with long rows (restriction, coarse Galerkin operators): one group of G lanes
-// per row, G = the power of two nearest the mean row length (4..32)
+// CSR for the rectangular transfer operators and the coarse Galerkin operators, processed in row
+// blocks: block b covers rows [rb[b].x, rb[b + 1].x) and entries [rb[b].y, rb[b + 1].y)
 template <typename T>
 struct DevCsr {
-    int n = 0, group = 32;
+    int n = 0, nblk = 0;
+    const int2* rb = nullptr;
+    int* err = nullptr;  // set to 1 when a staged copy never lands (never in a correct run)
     const int* ptr = nullptr;
     const int* col = nullptr;
     const T* val = nullptr;
@@ -42,6 +44,8 @@ struct DevCsr {
 
 // coarsest level: at most this many rows, inverted densely (2500^2 doubles = 50 MB)
 constexpr int COARSE_MAX = 2500;
+// largest coarsest level accepted when coarsening stops early (level cap)
+constexpr int DENSE_MAX = 4096;
 
 class Amg {
 public:
@@ -57,6 +61,8 @@ public:
     void vcycle(const double* b, double* z, cudaStream_t s);
     void vcycle(const float* b, float* z, cudaStream_t s);
     long long launches = 0;
+    // true when a cycle kernel gave up on a copy (the flag is cleared)
+    bool failed();
     // Recompute every value of the hierarchy on the device for a new finest-level operator with the
     // same sparsity: the aggregates, sparsity patterns and smoothing weights of setup() are kept
     // (a valid multigrid for any values; the captured cycle's device addresses do not change).
@@ -74,8 +80,8 @@ private:
         std::vector<double> val;
         // CSR copy used instead of the slices when rows are long
         bool csr = false;
-        int group = 32;
         std::vector<int> cptr, ccol;
+        std::vector<int> rb;  // row blocks: (first row, first entry) pairs, one past the last block included
         std::vector<double> cval;
     };
     struct Level {
@@ -94,7 +100,7 @@ private:
         // device
         DevBuf<long long> dA_soff, dP_soff, dR_soff;
         DevBuf<int> dA_w, dA_col, dP_w, dP_col, dR_w, dR_col;
-        DevBuf<int> cA_ptr, cA_col, cP_ptr, cP_col, cR_ptr, cR_col;
+        DevBuf<int> cA_ptr, cA_col, cP_ptr, cP_col, cR_ptr, cR_col, cA_rb, cP_rb, cR_rb;
         DevBuf<double> cA_v64, cP_v64, cR_v64;
         DevBuf<float> cA_v32, cP_v32, cR_v32;
         DevBuf<double> dA_v64, dP_v64, dR_v64, dinv64, x64, b64, r64, t64;
@@ -111,6 +117,7 @@ private:
 
     std::vector<Level> levels_;
     int ncoarse_ = 0;
+    DevBuf<int> err_;
     DevBuf<double> dinvc64_;  // dense inverse of the coarsest matrix
     DevBuf<float> dinvc32_;
 };

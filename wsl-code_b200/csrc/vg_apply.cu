@@ -33,6 +33,7 @@
 #include <algorithm>
 
 #include "vg_apply.cuh"
+#include "vg_pipe.cuh"
 
 namespace vg {
 
@@ -53,7 +54,6 @@ constexpr int CTAS_PER_SM = VG_CTAS_PER_SM;             // resident CTAs per SM 
 constexpr int BULK_THREADS = 32 * (BULK_CONSUMERS + 1);  // + one producer warp
 constexpr int MAX_STAGES = 4;
 constexpr int MAX_RING_BYTES = 200 << 10;                // dynamic shared memory of the ring
-constexpr unsigned long long WAIT_NS = 1000000000ull;    // 1 s: longer means a broken pipeline
 
 template <int NT>
 __device__ __forceinline__ void block_reduce2(double& a, double& b, double (*sh)[2]) {
@@ -374,75 +374,6 @@ __global__ void __launch_bounds__(APPLY_THREADS) apply_kernel(ApplyArgs<T> a) {
     double quad = 0, msum = 0;
     if (warp < a.npieces) piece_global<T, K>(a, a.pieces[warp], lane, quad, msum);
     if (a.red || a.mult) finish_reduction<T, APPLY_THREADS>(a, quad, msum);
-}
-
-// ---- shared-memory pipeline primitives (mbarrier + bulk copy, sm_90+ PTX) -------------------
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// L2 policy for data read once per apply (the operator records): evicted first, so the gathered
-// x and the scattered y stay resident in L2 while the records stream through
-__device__ __forceinline__ unsigned long long evict_first_policy() {
-    unsigned long long pol;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-
-// global -> shared bulk copy into this CTA, completing on an mbarrier; 16-byte aligned, size % 16 == 0
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* b,
-                                         unsigned long long pol) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
-            "r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(b)), "l"(pol)
-        : "memory");
-}
-
-__device__ __forceinline__ unsigned long long globaltimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// bounded wait for the phase of the given parity; false when it did not complete within WAIT_NS
-// (or an iteration cap), or when abort (optional) was raised by another thread of the CTA
-__device__ bool mbar_wait(unsigned long long* b, unsigned parity, const volatile int* abort) {
-    if (mbar_try_wait(b, parity)) return true;
-    const unsigned long long t0 = globaltimer();
-    for (unsigned it = 1; it < (1u << 24); ++it) {
-        if (mbar_try_wait(b, parity)) return true;
-        if ((it & 31u) == 0) {
-            if (abort && *abort) return false;
-            if (globaltimer() - t0 > WAIT_NS) return false;
-        }
-    }
-    return false;
 }
 
 template <typename T, int K>

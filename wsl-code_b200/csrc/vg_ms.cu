@@ -932,6 +932,8 @@ void Solver::ms_step(const double* old_state, double* new_state, const vg_solve_
     info.seconds = ms * 1e-3;
     n_iter += total;
     ++n_solve;
+    for (auto& a : ms_.amg)
+        if (a.ready() && a.failed()) throw Error(VG_ECUDA, "multigrid copy wait timed out");
     if (!(rel <= o.tol))
         throw Error(VG_ENOCONV, "Maxwell-Stefan step did not converge: iterations=" + std::to_string(total) +
                                     " true_relative_residual=" + std::to_string(rel));

@@ -891,6 +891,7 @@ void Solver::pack_streams(cudaStream_t s) {
 
 // the bulk-copy apply sets the error word when a pipeline wait gave up (never in a correct run)
 void Solver::check_pipeline() {
+    if (amg_.ready() && amg_.failed()) throw Error(VG_ECUDA, "multigrid copy wait timed out");
     if (k > 1) return;
     int e = 0;
     VG_CUDA(cudaMemcpy(&e, d_err_.data(), sizeof(int), cudaMemcpyDeviceToHost));
