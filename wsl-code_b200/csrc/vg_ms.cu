@@ -12,7 +12,8 @@
 // eliminated and B is frozen at x^n (one linear solve per step).
 //
 // B is not symmetric, so the system is solved by right-preconditioned GMRES(m) (classical
-// Gram-Schmidt applied twice, device vectors, Hessenberg and Givens rotations on the host), FP64 or
+// Gram-Schmidt applied twice; the Arnoldi loop of a cycle is a captured CUDA graph whose Hessenberg
+// column, Givens rotations and residual estimate are formed on the device), FP64 or
 // FP32 inner under FP64 iterative refinement, with a block-diagonal preconditioner: the 2x2 species
 // block of the assembled flux diagonal per flux dof, and for each species one smoothed-aggregation
 // V-cycle on its pressure Schur block (|E|/dt) I + W diag(F^{-1})_ss W^T (without the hierarchy:
