@@ -43,14 +43,17 @@ namespace {
 #define VG_BULK_CONSUMERS 8
 #endif
 #ifndef VG_STAGE_MIN_KB
-#define VG_STAGE_MIN_KB 24
+#define VG_STAGE_MIN_KB 24  // FP64 records; FP32 records use two thirds of it
 #endif
 #ifndef VG_CTAS_PER_SM
-#define VG_CTAS_PER_SM 2
+#define VG_CTAS_PER_SM 2  // FP64; FP32 (fewer registers per cell) runs one more CTA per SM
 #endif
 constexpr int BULK_CONSUMERS = VG_BULK_CONSUMERS;       // consumer warps per CTA
-constexpr int STAGE_MIN = VG_STAGE_MIN_KB << 10;        // smallest shared-memory stage
-constexpr int CTAS_PER_SM = VG_CTAS_PER_SM;             // resident CTAs per SM (k = 0)
+// smallest shared-memory stage and resident CTAs per SM (k = 0), by element size: measured at 1M
+// cells, FP32 runs 3 CTAs of 72 registers per thread with 16 KB stages (apply 39.0 -> 38.0 us),
+// FP64 stays at 2 CTAs of 96 registers (3 CTAs spill and take 70 us instead of 56)
+constexpr int stage_min(int elem_bytes) { return (elem_bytes == 4 ? 2 * VG_STAGE_MIN_KB / 3 : VG_STAGE_MIN_KB) << 10; }
+constexpr int ctas_per_sm(int elem_bytes) { return elem_bytes == 4 ? VG_CTAS_PER_SM + 1 : VG_CTAS_PER_SM; }
 constexpr int BULK_THREADS = 32 * (BULK_CONSUMERS + 1);  // + one producer warp
 constexpr int MAX_STAGES = 4;
 constexpr int MAX_RING_BYTES = 200 << 10;                // dynamic shared memory of the ring
@@ -377,7 +380,8 @@ __global__ void __launch_bounds__(APPLY_THREADS) apply_kernel(ApplyArgs<T> a) {
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(BULK_THREADS, K == 0 ? CTAS_PER_SM : 1) apply_bulk_kernel(ApplyArgs<T> a) {
+__global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(T))) : 1)
+    apply_bulk_kernel(ApplyArgs<T> a) {
     if (a.flags && a.flags[0]) return;  // solver converged: skip
     extern __shared__ __align__(128) unsigned char ring[];
     __shared__ __align__(8) unsigned long long full[MAX_STAGES], empty[MAX_STAGES];
@@ -492,14 +496,14 @@ StreamPlan plan_stream(const std::vector<Piece>& pieces, int k, int elem_bytes, 
         if (pieces[p].ne <= 9) common = std::max(common, rb);
     }
     pl.bytes = pl.rec_off[np];
-    // stage: at least STAGE_MIN and the largest record of a polygon with <= 9 edges; bigger records
+    // stage: at least stage_min and the largest record of a polygon with <= 9 edges; bigger records
     // (and anything above 96 KB) are read from the strided arrays
-    long long sb = std::max<long long>(STAGE_MIN, (common + 1023) / 1024 * 1024);
+    long long sb = std::max<long long>(stage_min(elem_bytes), (common + 1023) / 1024 * 1024);
     sb = std::min<long long>(sb, 96 << 10);
     pl.stage_bytes = int(sb);
     pl.stages = int(std::max<long long>(2, std::min<long long>(MAX_STAGES, MAX_RING_BYTES / sb)));
     const int per_sm = int(std::max<long long>(
-        1, std::min<long long>(k == 0 ? CTAS_PER_SM : 1, (227 << 10) / (pl.stages * sb + 8192))));
+        1, std::min<long long>(k == 0 ? ctas_per_sm(elem_bytes) : 1, (227 << 10) / (pl.stages * sb + 8192))));
     // batches: runs of whole records up to one stage
     ApplyBatch cur{0, 0, 0, 0, {0, 0, 0}};
     std::vector<long long> work;
