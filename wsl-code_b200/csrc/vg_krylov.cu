@@ -179,11 +179,11 @@ __global__ void __launch_bounds__(VEC_THREADS) k_init(const T* r, MinresVecs<T> 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(VEC_THREADS) k_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags,
-                                                        double* partials, unsigned* counter, long long plo,
-                                                        long long phi) {
+__global__ void __launch_bounds__(VEC_THREADS) k_update(MinresVecs<T> v, long long lo, long long hi, Scalars* sc,
+                                                        int* flags, double* partials, unsigned* counter,
+                                                        long long plo, long long phi, int reduce) {
     if (flags[0]) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) flags[1] = 0;
+        if (reduce && blockIdx.x == 0 && threadIdx.x == 0) flags[1] = 0;
         return;
     }
     const double g = sc->gam, gp = sc->gam_prev, dl = sc->delta / (g * g);
@@ -226,7 +226,8 @@ __global__ void __launch_bounds__(VEC_THREADS) k_update(MinresVecs<T> v, long lo
                 }
         }
     };
-    for_range(0, n, four, one);
+    for_range(lo, hi, four, one);
+    if (!reduce) return;
     const bool split = phi > plo;
     grid_reduce<1>(acc, partials, counter, [&](double* tot) {
         if (split)
@@ -351,8 +352,15 @@ void minres_init(const T* r, MinresVecs<T> v, long long n, Scalars* sc, int* fla
 template <typename T>
 void minres_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags, double* partials, unsigned* counter,
                    cudaStream_t s, long long plo, long long phi) {
+    minres_update_rows<T>(v, 0, n, 1, sc, flags, partials, counter, s, plo, phi);
+}
+
+template <typename T>
+void minres_update_rows(MinresVecs<T> v, long long lo, long long hi, int reduce, Scalars* sc, int* flags,
+                        double* partials, unsigned* counter, cudaStream_t s, long long plo, long long phi) {
     check_aligned(v);
-    k_update<T><<<VEC_BLOCKS, VEC_THREADS, 0, s>>>(v, n, sc, flags, partials, counter, plo, phi);
+    const int nb = reduce ? VEC_BLOCKS : int(std::min<long long>(VEC_BLOCKS, (hi - lo + 4 * VEC_THREADS - 1) / (4 * VEC_THREADS)));
+    k_update<T><<<std::max(nb, 1), VEC_THREADS, 0, s>>>(v, lo, hi, sc, flags, partials, counter, plo, phi, reduce);
     VG_CUDA(cudaGetLastError());
 }
 
@@ -376,6 +384,10 @@ template void minres_init<double>(const double*, MinresVecs<double>, long long, 
                                   unsigned*, cudaStream_t, long long, long long);
 template void minres_init<float>(const float*, MinresVecs<float>, long long, Scalars*, int*, double, double*,
                                  unsigned*, cudaStream_t, long long, long long);
+template void minres_update_rows<double>(MinresVecs<double>, long long, long long, int, Scalars*, int*, double*,
+                                         unsigned*, cudaStream_t, long long, long long);
+template void minres_update_rows<float>(MinresVecs<float>, long long, long long, int, Scalars*, int*, double*,
+                                        unsigned*, cudaStream_t, long long, long long);
 template void minres_update<double>(MinresVecs<double>, long long, Scalars*, int*, double*, unsigned*, cudaStream_t,
                                     long long, long long);
 template void minres_update<float>(MinresVecs<float>, long long, Scalars*, int*, double*, unsigned*, cudaStream_t,

@@ -33,6 +33,11 @@ void minres_init(const T* r, MinresVecs<T> v, long long n, Scalars* sc, int* fla
 template <typename T>
 void minres_update(MinresVecs<T> v, long long n, Scalars* sc, int* flags, double* partials, unsigned* counter,
                    cudaStream_t s, long long plo = 0, long long phi = 0);
+// the same on rows [lo, hi) only; reduce = 0: no dot product and no scalar update (a part of the
+// rows processed beside another launch that reduces)
+template <typename T>
+void minres_update_rows(MinresVecs<T> v, long long lo, long long hi, int reduce, Scalars* sc, int* flags,
+                        double* partials, unsigned* counter, cudaStream_t s, long long plo, long long phi);
 // gamma^2 over [plo, phi) + the partial of init / update, then the scalar recurrences
 template <typename T>
 void minres_finish(const T* z, const T* v, long long plo, long long phi, Scalars* sc, int* flags, double* partials,

@@ -279,6 +279,9 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
     VG_CUDA(cudaEventCreate(&ev1_));
     VG_CUDA(cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming));
     VG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    VG_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    VG_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+    VG_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
     d_loop_.resize(2);
 }
 
@@ -289,6 +292,9 @@ Solver::~Solver() {
     if (ev1_) cudaEventDestroy(ev1_);
     if (ev_in_) cudaEventDestroy(ev_in_);
     if (stream_) cudaStreamDestroy(stream_);
+    if (side_) cudaStreamDestroy(side_);
+    if (ev_fork_) cudaEventDestroy(ev_fork_);
+    if (ev_join_) cudaEventDestroy(ev_join_);
 }
 
 void Solver::destroy_graphs() {
@@ -967,8 +973,21 @@ void Solver::iteration(MinresVecs<T>& v, cudaStream_t s) {
     int* flags = d_flags_.data();
     const long long plo = use_amg ? nf : 0, phi = use_amg ? nf + np : 0;
     launch_apply(apply_args<T>(v.z_cur, v.y, true, T(-1), &sc->delta, flags), s);
-    minres_update<T>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s, plo, phi);
-    if (use_amg) {
+    if (use_amg && phi == N) {
+        // the flux rows of the update (bandwidth-bound) run on a second stream beside the pressure
+        // rows and the V-cycle (latency-bound); both join before the scalar update
+        VG_CUDA(cudaEventRecord(ev_fork_, s));
+        VG_CUDA(cudaStreamWaitEvent(side_, ev_fork_, 0));
+        minres_update_rows<T>(v, 0, plo, 1, sc, flags, d_partials_.data(), d_counter_.data(), side_, plo, phi);
+        VG_CUDA(cudaEventRecord(ev_join_, side_));
+        minres_update_rows<T>(v, plo, phi, 0, sc, flags, d_partials_.data(), d_counter_.data(), s, plo, phi);
+        amg_.vcycle(v.v_old + nf, v.z_new + nf, s);
+        VG_CUDA(cudaStreamWaitEvent(s, ev_join_, 0));
+        minres_finish<T>(v.z_new, v.v_old, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(), 0, 0.0, s);
+    } else {
+        minres_update<T>(v, N, sc, flags, d_partials_.data(), d_counter_.data(), s, plo, phi);
+    }
+    if (use_amg && phi != N) {
         amg_.vcycle(v.v_old + nf, v.z_new + nf, s);
         minres_finish<T>(v.z_new, v.v_old, plo, phi, sc, flags, d_partials_.data(), d_counter_.data(), 0, 0.0, s);
     }

@@ -197,6 +197,8 @@ private:
     DevBuf<float> sv32_[2];
     DevBuf<int> d_loop_;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t side_ = nullptr;  // second branch of a MINRES iteration (flux rows of the update)
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     cudaEvent_t ev_in_ = nullptr;
     cudaGraph_t graph_[2] = {nullptr, nullptr};
     cudaGraphExec_t gexec_[2] = {nullptr, nullptr};
