@@ -485,10 +485,6 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
     }
 }
 
-// CTAs resident per SM of the CSR kernels (shared memory bound), set once
-int g_csr_ctas[2] = {0, 0};  // FP32, FP64
-int g_sm_count = 0;
-
 template <int OP, typename T>
 void prepare_csr_op() {
     VG_CUDA(cudaFuncSetAttribute(k_csr<OP, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, CsrSmem<T>::total));
@@ -497,8 +493,9 @@ void prepare_csr_op() {
                                  int(cudaSharedmemCarveoutMaxShared)));
 }
 
-void prepare_csr_kernels() {
-    if (g_sm_count) return;
+// kernel attributes on the current device (function attributes are per device) and the number of
+// CTAs of each precision's CSR kernel the device holds at once: slots[0] FP32, slots[1] FP64
+void prepare_csr_kernels(int slots[2]) {
     prepare_csr_op<0, float>();
     prepare_csr_op<1, float>();
     prepare_csr_op<2, float>();
@@ -512,16 +509,15 @@ void prepare_csr_kernels() {
     VG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n32, k_csr<3, float>, TPB, CsrSmem<float>::total));
     VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n64, k_csr<3, double>, TPB, CsrSmem<double>::total));
-    g_csr_ctas[0] = std::max(1, n32);
-    g_csr_ctas[1] = std::max(1, n64);
-    g_sm_count = std::max(1, sms);
+    slots[0] = std::max(1, n32) * std::max(1, sms);
+    slots[1] = std::max(1, n64) * std::max(1, sms);
 }
 
 template <typename T>
 void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, const T* x, T* y, T* r,
                 cudaStream_t s) {
     if (M.n <= 0 || M.nblk <= 0) return;
-    const int grid = std::min(M.nblk, g_sm_count * g_csr_ctas[sizeof(T) == 8 ? 1 : 0]);
+    const int grid = std::min(M.nblk, std::max(1, M.slots));
     const int sb = CsrSmem<T>::total;
     switch (op) {
     case 0: launch_pdl(k_csr<0, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
@@ -999,7 +995,7 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
     }
     err_.resize(1);
     err_.zero();
-    prepare_csr_kernels();
+    prepare_csr_kernels(csr_slots_);
     pt.mark("multigrid uploads");
 }
 
@@ -1028,6 +1024,7 @@ DevCsr<T> Amg::cview(const Level& L, int which) const {
     const Sell& S = which == 0 ? L.A : which == 1 ? L.P : L.R;
     v.n = S.n;
     v.nblk = S.csr ? int(S.rb.size() / 2) - 1 : 0;
+    v.slots = csr_slots_[sizeof(T) == 8 ? 1 : 0];
     v.err = const_cast<int*>(err_.data());
     v.rb = reinterpret_cast<const int2*>((which == 0 ? L.cA_rb : which == 1 ? L.cP_rb : L.cR_rb).data());
     v.ptr = (which == 0 ? L.cA_ptr : which == 1 ? L.cP_ptr : L.cR_ptr).data();

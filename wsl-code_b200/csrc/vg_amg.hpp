@@ -35,6 +35,7 @@ struct DevSell {
 template <typename T>
 struct DevCsr {
     int n = 0, nblk = 0;
+    int slots = 1;  // CTAs of the kernel resident at once on the device (grid cap)
     const int2* rb = nullptr;
     int* err = nullptr;  // set to 1 when a staged copy never lands (never in a correct run)
     const int* ptr = nullptr;
@@ -118,6 +119,7 @@ private:
     std::vector<Level> levels_;
     int ncoarse_ = 0;
     DevBuf<int> err_;
+    int csr_slots_[2] = {1, 1};  // resident CTAs of the CSR kernels on this hierarchy's device (FP32, FP64)
     DevBuf<double> dinvc64_;  // dense inverse of the coarsest matrix
     DevBuf<float> dinvc32_;
 };
