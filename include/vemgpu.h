@@ -91,7 +91,8 @@ typedef struct vg_solve_opts {
     int mode;            /* VG_SOLVE_FP64 or VG_SOLVE_MIXED                                    */
     double tol;          /* relative true residual ||b - A x|| / ||b|| (reference: 1e-10)      */
     int maxit;           /* cap on total inner iterations                                      */
-    double inner_tol;    /* MIXED: relative reduction asked of each FP32 inner solve           */
+    double inner_tol;    /* MIXED: relative reduction asked of each FP32 inner solve (a later
+                            step asks for less, 0.1 tol / current residual, when that suffices) */
     int max_outer;       /* MIXED: cap on refinement steps                                     */
     int check_every;     /* 0: the whole Krylov loop is one CUDA graph (device-side while node,
                             iteration cap on the device); > 0: host-driven batches of this many

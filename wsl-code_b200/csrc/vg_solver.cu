@@ -1139,7 +1139,10 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
             to_float(r.data(), r32.data(), 1.0 / rn, N, s);
             n_launch += 2;
             int it = 0;
-            minres(true, r32.data(), d32.data(), o.inner_tol, o.maxit - total, o.check_every, it, s);
+            // reduction asked of this FP32 solve: inner_tol, or less when less reaches tol (with the
+            // same 0.1 margin as the FP64 path)
+            const double itol = std::min(0.5, std::max(o.inner_tol, 0.1 * o.tol / rel));
+            minres(true, r32.data(), d32.data(), itol, o.maxit - total, o.check_every, it, s);
             total += it;
             axpy_from_float(x, d32.data(), rn, N, s);
             rel = true_residual();
