@@ -290,7 +290,7 @@ __device__ void ms_grid_sum(double (*sh)[MS_MAXM], int cnt, double* partials, un
 }
 
 // out[k] = V[:, k] . w for k < cnt, cnt = (cnt_dev ? *cnt_dev : 0) + cnt_add. Block b stages its
-// rows of w in shared memory and streams the cnt columns over them (two at a time, 16-byte
+// rows of w in shared memory and streams the cnt columns over them (four at a time, 16-byte
 // loads); the column stride ld and chunk are multiples of 4.
 template <typename T>
 __global__ void __launch_bounds__(MS_THREADS) k_mdot(const T* V, long long ld, const int* cnt_dev, int cnt_add,
@@ -311,31 +311,45 @@ __global__ void __launch_bounds__(MS_THREADS) k_mdot(const T* V, long long ld, c
     for (int i = len4 + threadIdx.x; i < len; i += MS_THREADS) ws[i] = w[lo + i];
     __syncthreads();
     const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
-    for (int k = 0; k < cnt; k += 2) {
-        const bool two = k + 1 < cnt;
+    // four columns at a time, rows unrolled by two: about eight 16-byte loads in flight per thread
+    for (int k = 0; k < cnt; k += 4) {
+        const int nk = min(4, cnt - k);
         const T* v0 = V + k * ld + lo;
-        const T* v1 = two ? v0 + ld : v0;
-        double a0 = 0, a1 = 0;
+        const T* v1 = nk > 1 ? v0 + ld : v0;
+        const T* v2 = nk > 2 ? v0 + 2 * ld : v0;
+        const T* v3 = nk > 3 ? v0 + 3 * ld : v0;
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
 #pragma unroll 2
         for (int i = 4 * threadIdx.x; i < len4; i += 4 * MS_THREADS) {
-            T x[4], p[4], q[4];
+            T x[4], p0[4], p1[4], p2[4], p3[4];
+            ld4(v0 + i, p0);
+            ld4(v1 + i, p1);
+            ld4(v2 + i, p2);
+            ld4(v3 + i, p3);
             ld4(ws + i, x);
-            ld4(v0 + i, p);
-            ld4(v1 + i, q);
-            a0 += dot4(p, x);
-            a1 += dot4(q, x);
+            a0 += dot4(p0, x);
+            a1 += dot4(p1, x);
+            a2 += dot4(p2, x);
+            a3 += dot4(p3, x);
         }
         for (int i = len4 + threadIdx.x; i < len; i += MS_THREADS) {
-            a0 += double(v0[i]) * double(ws[i]);
-            a1 += double(v1[i]) * double(ws[i]);
+            const double xi = double(ws[i]);
+            a0 += double(v0[i]) * xi;
+            a1 += double(v1[i]) * xi;
+            a2 += double(v2[i]) * xi;
+            a3 += double(v3[i]) * xi;
         }
         for (int off = 16; off; off >>= 1) {
             a0 += __shfl_down_sync(0xffffffffu, a0, off);
             a1 += __shfl_down_sync(0xffffffffu, a1, off);
+            a2 += __shfl_down_sync(0xffffffffu, a2, off);
+            a3 += __shfl_down_sync(0xffffffffu, a3, off);
         }
         if (l == 0) {
             sh[wid][k] = a0;
-            if (two) sh[wid][k + 1] = a1;
+            if (nk > 1) sh[wid][k + 1] = a1;
+            if (nk > 2) sh[wid][k + 2] = a2;
+            if (nk > 3) sh[wid][k + 3] = a3;
         }
     }
     __syncthreads();
