@@ -651,9 +651,16 @@ void Solver::ms_precond(const T* r, T* z) {
     const T* C = sizeof(T) == 8 ? reinterpret_cast<const T*>(ms_.C64.data()) : reinterpret_cast<const T*>(ms_.C32.data());
     k_ms_pc_apply<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(r, z, F, C, nf, m.nc);
     VG_CUDA(cudaGetLastError());
-    if (ms_.amg_ready)  // pressure blocks: one V-cycle per species (replaces the 2x2 cell blocks)
-        for (int s = 0; s < 2; ++s)
-            ms_.amg[s].vcycle(r + 2 * nf + (long long)s * m.nc, z + 2 * nf + (long long)s * m.nc, stream_);
+    if (ms_.amg_ready) {  // pressure blocks: one V-cycle per species (replaces the 2x2 cell blocks)
+        // the two species' cycles are independent chains of small kernels: the second runs on a
+        // second stream beside the first
+        VG_CUDA(cudaEventRecord(ev_fork_, stream_));
+        VG_CUDA(cudaStreamWaitEvent(side_, ev_fork_, 0));
+        ms_.amg[1].vcycle(r + 2 * nf + m.nc, z + 2 * nf + m.nc, side_);
+        VG_CUDA(cudaEventRecord(ev_join_, side_));
+        ms_.amg[0].vcycle(r + 2 * nf, z + 2 * nf, stream_);
+        VG_CUDA(cudaStreamWaitEvent(stream_, ev_join_, 0));
+    }
 }
 
 // S_s = diag(|E|/dt) + W diag((F_g^{-1})_ss) W^T on the cell graph (k = 0: W = +-1 per local edge,
