@@ -214,7 +214,7 @@ int vg_ms_configure(vg_handle* h, double d12, double d13, double d23, double dt,
 /* y = K(coeff_state) x for the Maxwell-Stefan system (FP64 or FP32 x, y; device). */
 int vg_ms_apply(vg_handle* h, const double* coeff_state, const void* x, void* y, int precision);
 /* One backward-Euler step: solve K(old) new = [0; |E|/dt x_old] to ||b - K new|| / ||b|| <= opts->tol
- * by right-preconditioned GMRES(30), FP64 or FP32 inner under FP64 refinement (opts->mode). */
+ * by right-preconditioned GMRES(10), FP64 or FP32 inner under FP64 refinement (opts->mode). */
 int vg_ms_step(vg_handle* h, const double* old_state, double* new_state, const vg_solve_opts* opts,
                vg_solve_info* info);
 
