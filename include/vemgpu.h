@@ -112,7 +112,10 @@ typedef struct vg_solve_info {
 /* Processed mesh (the reference reader's output). k in 0..4, nq in {1,3,4,7,9,12,36},
  * ng in [k+2, 10], with the reference's consistency rules (vem/CurvedVEM_Darcy_gpu/src/solver_options.cpp:123-136).
  * Replaces HdivGpu::HdivGpu (vem/CurvedVEM_Darcy_gpu/include/hdiv_gpu.cuh:55-56) and
- * HostMesh::HostMesh (vem/CurvedVEM_Darcy_gpu/src/mesh_pack.cpp:127-238). device < 0: current device. */
+ * HostMesh::HostMesh (vem/CurvedVEM_Darcy_gpu/src/mesh_pack.cpp:127-238). device < 0: current device.
+ * The caller's current device is the same on return; every later call on the handle runs on the
+ * handle's device and gives the caller's current device back (one thread may hold handles on
+ * several GPUs). */
 int vg_create(const vg_mesh* mesh, const vg_geometry* geometry, int k, int nq, int ng, int device, vg_handle** out);
 
 /* Raw polygons (any orientation): performs the reader post-processing of
@@ -221,7 +224,9 @@ int vg_ms_step(vg_handle* h, const double* old_state, double* new_state, const v
 /* ---- post-processing ---------------------------------------------------------------------- */
 
 /* Six figures of MixedGpu::errors (equation_gpu.cu:387-479, 627-648): computational scalar and
- * flux L2 errors, physical scalar, flux and divergence L2 errors, physical mean-pressure mass. */
+ * flux L2 errors, physical scalar, flux and divergence L2 errors, physical mean-pressure mass.
+ * Runs on the legacy default stream, which does not wait for work queued on non-blocking streams
+ * (torch's side streams are non-blocking): synchronize the stream that wrote x before the call. */
 int vg_errors(vg_handle* h, const double* x, double out[6]);
 
 /* vg_errors without any device allocation: the per-cell figures and their sums live in a
@@ -229,11 +234,12 @@ int vg_errors(vg_handle* h, const double* x, double out[6]);
  * VG_EINVAL. For callers that must not allocate device memory between solves: a process whose
  * HBM is already reserved by its own caching allocator (cudaMalloc may fail there), or one that
  * monitors the error inside a loop while other streams run (cudaMalloc and cudaFree can
- * synchronize the device). Same results as vg_errors. The first call on a device looks up the
- * array's address and must come before any stream capture on that device. The array is shared
- * by every handle of a device, so calls that overlap on the GPU (several host threads) race.
- * Runs on the legacy default stream and returns after the figures are on the host.
- * No counterpart in the reference. */
+ * synchronize the device). Same results as vg_errors. Every call looks up the array's device
+ * address (no allocation); the first call on a device may load the library's device code and must
+ * come before any stream capture on that device. The array is shared by every handle of a device,
+ * so calls that overlap on the GPU (several host threads) race. Runs on the legacy default stream,
+ * like vg_errors (synchronize the stream that wrote x before the call), and returns after the
+ * figures are on the host. No counterpart in the reference. */
 #define VG_ERRORS_NOALLOC_MAX_CELLS 262144
 int vg_errors_noalloc(vg_handle* h, const double* x, double out[6]);
 

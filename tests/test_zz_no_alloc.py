@@ -1,6 +1,8 @@
 """vg_errors_noalloc (static device scratch, no device allocation) against vg_errors, through the
 C ABI. The figures come from the same kernels and the same fixed-order reduction, so they must
-agree bit for bit, on repeated calls and across handles that reuse the same static scratch."""
+agree bit for bit, on repeated calls and across handles that reuse the same static scratch, and
+the entry point must keep working when the device has no memory left to allocate (the situation
+of a caller whose caching allocator holds all of HBM)."""
 import ctypes
 
 import numpy as np
@@ -63,4 +65,40 @@ def test_noalloc_rejects_meshes_above_limit():
     assert "VG_ERRORS_NOALLOC_MAX_CELLS" in str(e.value)
     # the ordinary entry point still works on the same handle
     assert np.all(np.isfinite(_figures(g, x, "vg_errors")))
+    g.close()
+
+
+def test_noalloc_works_with_device_memory_exhausted():
+    """With every free byte of the device taken, vg_errors (which allocates its per-cell scratch)
+    returns VG_ENOMEM while vg_errors_noalloc still returns the same figures, twice in a row."""
+    from cuda.bindings import runtime as rt
+    n = 440  # 193,600 cells: vg_errors asks for 6 * 193,600 doubles = 9.3 MB of scratch
+    g = vemgpu.DarcyGpu(_grid(n), k=0, geometry="identity", problem="sincos", bc="flux")
+    x = torch.randn(g.N, dtype=torch.float64, device="cuda")
+    ref = _figures(g, x, "vg_errors")
+    assert np.array_equal(_figures(g, x, "vg_errors_noalloc"), ref)  # loads the kernels first
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    held = []
+    try:
+        # take the device's free memory in decreasing blocks, down to 2 MB
+        size = 1 << 30
+        while size >= (2 << 20):
+            err, ptr = rt.cudaMalloc(size)
+            if err == rt.cudaError_t.cudaSuccess:
+                held.append(ptr)
+            else:
+                rt.cudaGetLastError()
+                size //= 2
+        err, free, _ = rt.cudaMemGetInfo()
+        assert err == rt.cudaError_t.cudaSuccess and free < 6 * 8 * g.nc, free
+        with pytest.raises(L.VemGpuError) as e:
+            _figures(g, x, "vg_errors")
+        assert e.value.code == L.VG_ENOMEM
+        for _ in range(2):
+            assert np.array_equal(_figures(g, x, "vg_errors_noalloc"), ref)
+    finally:
+        for ptr in held:
+            rt.cudaFree(ptr)
+    assert np.array_equal(_figures(g, x, "vg_errors"), ref)
     g.close()

@@ -15,10 +15,44 @@ struct vg_handle {
 namespace {
 thread_local std::string g_create_error;
 
+// Makes a device current for the duration of a call and gives the caller's current device back
+// afterwards: a thread may hold handles on several GPUs, and every handle's buffers, streams and
+// kernels belong to the device it was created on.
+class DeviceScope {
+    int prev_ = -1;
+    bool switched_ = false, restore_only_ = false;
+
+public:
+    // device < 0: only remember the current device (nothing to restore when there is none)
+    explicit DeviceScope(int device) {
+        if (device < 0) {
+            if (cudaGetDevice(&prev_) == cudaSuccess)
+                restore_only_ = true;
+            else
+                cudaGetLastError();
+            return;
+        }
+        VG_CUDA(cudaGetDevice(&prev_));
+        if (device != prev_) {
+            VG_CUDA(cudaSetDevice(device));
+            switched_ = true;
+        }
+    }
+    ~DeviceScope() {
+        if (switched_ || restore_only_) {
+            int cur = -1;
+            if (cudaGetDevice(&cur) == cudaSuccess && cur != prev_) cudaSetDevice(prev_);
+        }
+    }
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
 template <class F>
 int guarded(vg_handle* h, F f) {
     if (!h || !h->s) return VG_EINVAL;
     try {
+        DeviceScope scope(h->s->device());
         f(*h->s);
         h->error.clear();
         return VG_OK;
@@ -36,6 +70,7 @@ int guarded(vg_handle* h, F f) {
 
 int create(vg::HostMesh&& m, const vg_geometry* g, int k, int nq, int ng, int device, vg_handle** out) {
     auto h = std::make_unique<vg_handle>();
+    DeviceScope scope(-1);  // the constructor selects `device`; the caller's device comes back after it
     h->s = std::make_unique<vg::Solver>(std::move(m), g, k, nq, ng, device);
     *out = h.release();
     return VG_OK;
@@ -101,6 +136,14 @@ int vg_create_vtk(const char* path, const vg_geometry* geometry, int k, int nq, 
 }
 
 int vg_destroy(vg_handle* h) {
+    if (h && h->s) {
+        try {
+            DeviceScope scope(h->s->device());  // the buffers are freed on their own device
+            h->s.reset();
+        } catch (...) {
+            h->s.reset();
+        }
+    }
     delete h;
     return VG_OK;
 }

@@ -3,7 +3,6 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <unordered_map>
 
 #include "vg_apply.cuh"
@@ -1301,43 +1300,33 @@ namespace {
 constexpr long long kErrScratch = 6LL * VG_ERRORS_NOALLOC_MAX_CELLS + 8;
 static __device__ __align__(256) double g_err_scratch[kErrScratch];
 
-// device address of g_err_scratch, looked up once per device with that device current
-double* err_scratch(int device) {
-    static std::mutex mu;
-    static std::unordered_map<int, double*> addr;
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = addr.find(device);
-    if (it != addr.end()) return it->second;
+// device address of g_err_scratch on the current device. Looked up on every call (the lookup
+// allocates nothing and is cheap): an address kept across calls would go stale when the device's
+// primary context is reset and created again in the same process.
+double* err_scratch() {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_err_scratch);
-    if (e != cudaSuccess || !p)
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
         throw Error(VG_ECUDA, std::string("cudaGetSymbolAddress(error scratch): ") + cudaGetErrorString(e));
-    addr[device] = static_cast<double*>(p);
+    }
     return static_cast<double*>(p);
 }
 }  // namespace
 
+// The C ABI makes the handle's device current before this runs (DeviceScope in vg_capi.cu).
 void Solver::errors_static(const double* x, double out[6]) {
     if (!built) throw Error(VG_ESTATE, "vg_build must run before vg_errors_noalloc");
     if (m.nc > VG_ERRORS_NOALLOC_MAX_CELLS)
         throw Error(VG_EINVAL, "vg_errors_noalloc: " + std::to_string(m.nc) +
                                    " cells exceed the static scratch limit VG_ERRORS_NOALLOC_MAX_CELLS = " +
                                    std::to_string(VG_ERRORS_NOALLOC_MAX_CELLS));
-    int cur = -1;
-    VG_CUDA(cudaGetDevice(&cur));
-    if (cur != device_) VG_CUDA(cudaSetDevice(device_));
-    try {
-        double* per = err_scratch(device_);
-        double* sum = per + 6LL * VG_ERRORS_NOALLOC_MAX_CELLS;
-        for (const auto& c : classes_) launch_errors(setup_args_, c, nq, x, per, nullptr);
-        launch_error_sum(per, m.nc, sum, nullptr);
-        VG_CUDA(cudaMemcpyAsync(out, sum, 6 * sizeof(double), cudaMemcpyDeviceToHost, nullptr));
-        VG_CUDA(cudaStreamSynchronize(nullptr));
-    } catch (...) {
-        if (cur != device_) cudaSetDevice(cur);
-        throw;
-    }
-    if (cur != device_) VG_CUDA(cudaSetDevice(cur));
+    double* per = err_scratch();
+    double* sum = per + 6LL * VG_ERRORS_NOALLOC_MAX_CELLS;
+    for (const auto& c : classes_) launch_errors(setup_args_, c, nq, x, per, nullptr);
+    launch_error_sum(per, m.nc, sum, nullptr);
+    VG_CUDA(cudaMemcpyAsync(out, sum, 6 * sizeof(double), cudaMemcpyDeviceToHost, nullptr));
+    VG_CUDA(cudaStreamSynchronize(nullptr));
 }
 
 int Solver::local(int cell, int which, double* out) {

@@ -67,6 +67,7 @@ public:
     template <typename T>
     void ms_apply(const T* x, T* y);
     long long ms_size() const { return ms_.N; }
+    int device() const { return device_; }  // the CUDA device that holds this handle's data
     void cell_areas(double* out);
     // assembled CSR of the system (comparator of the matrix-free apply); rp == nullptr: size only
     void assemble(int constrained, long long* nnz, long long* rp, int* ci, double* val);
