@@ -155,8 +155,18 @@ int vg_build(vg_handle* h);
 /* y = A x, reference sign [A, -W^T, 0; W, 0, L; 0, L^T, 0], device pointers (x != y).
  * precision VG_FP64 (double*) or VG_FP32 (float*). constrained = 1 applies the essential-BC mask
  * as Q A Q + (I - Q) (VG_BC_FLUX only). stream: cudaStream_t or NULL (legacy default stream).
+ * Asynchronous: a failure inside the kernel (a copy-pipeline wait that gave up; never in a correct
+ * run) is reported as VG_ECUDA by a later vg_apply on the handle, once the error word's copy has
+ * reached the host, or by the next vg_solve.
  * Replaces MixedGpu::apply (vem/CurvedVEM_Darcy_gpu/src/equation_gpu.cu:580-598). */
 int vg_apply(vg_handle* h, const void* x, void* y, int precision, int constrained, void* stream);
+
+/* Failure-path test hook (no counterpart in the reference): the next matrix-free apply of the
+ * handle (k <= 1) leaves one operator batch uncopied, so that the waits of the CTA that owns it
+ * run out after their one-second limit; the kernel then drains its copies, sets its error word and
+ * returns, and the call that launched it reports VG_ECUDA as described for vg_apply and vg_solve.
+ * The result of that apply is wrong. For tests of the error path only. */
+int vg_debug_stall_apply(vg_handle* h);
 
 /* Internally the solver numbers the flux unknowns by first use in its cell layout and the pressure
  * rows by cell layout, so that the apply's gathers and scatters coalesce; vg_apply and vg_solve

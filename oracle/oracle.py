@@ -32,10 +32,7 @@ _lib = None
 
 def build():
     """Compile liboracle.so (and oracle/_ref when the reference checkout is present)."""
-    targets = ["all"]
-    if os.path.isdir("/root/reference/vem/CurvedVEM_Darcy_gpu"):
-        targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "all", "ref-if-present"], check=True)
 
 
 def lib():
@@ -58,6 +55,7 @@ def lib():
         L.orc_samples.restype = ctypes.c_long
         L.orc_samples.argtypes = [P, I, I, P]
         L.orc_errors.argtypes = [P, P, P]
+        L.orc_adjoint_contract.argtypes = [P, P, P, P, P]
         L.orc_gmres_ilu.restype = I
         L.orc_gmres_ilu.argtypes = [I, P, P, P, P, P, D, I, I, P]
         L.orc_reference_solve.restype = I
@@ -177,6 +175,15 @@ class Oracle:
         lib().orc_errors(self.h, x.ctypes.data, out.ctypes.data)
         return dict(scalar_comp=out[0], flux_comp=out[1], scalar_phys=out[2], flux_phys=out[3],
                     div_phys=out[4], mass=out[5])
+
+    def adjoint_contract(self, x, lam, mask=None):
+        """Per-cell g_E = (S_E lam_E)^T A_E (S_E x_E), lam zero on masked rows (CPU FP64)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.int32)
+        g = np.zeros(self.nc)
+        lib().orc_adjoint_contract(self.h, x.ctypes.data, lam.ctypes.data, _p(m), g.ctypes.data)
+        return g
 
     def solve_direct(self):
         """Golden discrete solution: sparse LU on the reduced system (free dofs)."""

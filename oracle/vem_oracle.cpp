@@ -1294,6 +1294,26 @@ long orc_samples(void* h, int c, int edge, double* out) {
 
 void orc_errors(void* h, const double* x, double* out6) { static_cast<Oracle*>(h)->errors(x, out6); }
 
+// Adjoint contraction per cell, g_E = (S_E lam_E)^T A_E (S_E x_E) over the local flux dofs, S_E the
+// orientation signs and lam zero on masked (essential) rows (mask may be null): the CPU FP64
+// counterpart of the GPU gradient dJ/dtheta_E = lambda_E^T A_E(theta) u_E (A_E = e^{-theta_E} A_E(0)).
+void orc_adjoint_contract(void* h, const double* x, const double* lam, const int* mask, double* g) {
+    auto* o = static_cast<Oracle*>(h);
+    for (int c = 0; c < o->m.nc; ++c) {
+        const int nn = o->n[c];
+        const auto& gd = o->gdofs[c];
+        const auto& dr = o->dir[c];
+        double acc = 0;
+        for (int i = 0; i < nn; ++i) {
+            const double li = (mask && mask[gd[i]]) ? 0.0 : dr[i] * lam[gd[i]];
+            double row = 0;
+            for (int j = 0; j < nn; ++j) row += o->A[c][i * nn + j] * dr[j] * x[gd[j]];
+            acc += li * row;
+        }
+        g[c] = acc;
+    }
+}
+
 // GMRES(restart) + ILU(0) on a CSR matrix (left preconditioning, preconditioned residual norm)
 int orc_gmres_ilu(int n, const int* ptr, const int* col, const double* val, const double* b, double* x, double rtol,
                   int restart, int maxit, double* rel_out) {

@@ -30,7 +30,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle as O  # noqa: E402
 
-REF = "/root/reference/vem"
+# root of the reference checkout (environment variable REFERENCE, same name as in oracle/Makefile)
+REFERENCE = os.environ.get("REFERENCE", "/root/reference")
+REF = os.path.join(REFERENCE, "vem")
 GPU = REF + "/CurvedVEM_Darcy_gpu"
 CPU = REF + "/CurvedVEM_Darcy"
 MESHES = ["square_1x1", "square_2x2", "square_4x4", "square_8x8", "square_16x16", "square_32x32"]
@@ -76,7 +78,7 @@ def table(path, k, nq, cols):
                 continue
             vals = {name: float(t[i]) for name, i in cols.items()}
             rows.append(dict(mesh=t[0], line=lineno, **vals))
-    return dict(source=os.path.relpath(path, "/root/reference"), k=k, example=1, nq=nq, ng=9, rows=rows)
+    return dict(source=os.path.relpath(path, REFERENCE), k=k, example=1, nq=nq, ng=9, rows=rows)
 
 
 def tables():
@@ -103,7 +105,7 @@ def k3_table():
             if section and t and t[0] in MESHES:
                 rows.setdefault(t[0], dict(mesh=t[0], dofs=float(t[1])))[section] = float(t[2])
                 rows[t[0]]["line_" + section] = lineno
-    return dict(source=os.path.relpath(path, "/root/reference"), k=3, example=1, nq=12, ng=9,
+    return dict(source=os.path.relpath(path, REFERENCE), k=3, example=1, nq=12, ng=9,
                 rows=list(rows.values()))
 
 

@@ -320,3 +320,29 @@ def test_multigrid_high_order_pressure_bc(k):
     x, info = g.solve(tol=1e-10)
     assert info["residual"] <= 1e-10
     assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+
+
+def test_calls_run_on_the_handles_device():
+    """Every call runs on the device the handle was created on and leaves the caller's current
+    device as it was (with one GPU both are device 0)."""
+    import ctypes
+    from vemgpu import _lib as L
+    other = 1 if torch.cuda.device_count() > 1 else 0
+    torch.cuda.set_device(other)
+    try:
+        m = meshgen.voronoi_mesh(1000, "disk", seed=2)
+        g = vemgpu.DarcyGpu(m, k=0, geometry="arcs", problem="sinsin", bc="pressure", device=0)
+        assert torch.cuda.current_device() == other
+        b = torch.zeros(g.N, dtype=torch.float64, device="cuda:0")
+        x = torch.zeros_like(b)
+        L.check(L.lib().vg_rhs(g.h, b.data_ptr()), g.h)
+        assert torch.cuda.current_device() == other
+        o = g.opts(tol=1e-10)
+        info = L.VgSolveInfo()
+        L.check(L.lib().vg_solve(g.h, b.data_ptr(), x.data_ptr(), ctypes.byref(o), ctypes.byref(info)), g.h)
+        assert torch.cuda.current_device() == other
+        assert info.residual <= 1e-10
+        g.close()
+        assert torch.cuda.current_device() == other
+    finally:
+        torch.cuda.set_device(0)

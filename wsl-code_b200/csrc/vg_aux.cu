@@ -260,6 +260,12 @@ __global__ void k_axpy64(double* x, const double* d, double a, long long n) {
         x[i] += a * d[i];
 }
 
+// smallest index of a non-finite entry (atomicMin into *first, which starts at n)
+__global__ void k_first_nonfinite(const double* v, long long n, unsigned long long* first) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (!isfinite(v[i])) atomicMin(first, (unsigned long long)i);
+}
+
 inline int blocks_for(long long n) { return int((n + 255) / 256); }
 
 }  // namespace
@@ -337,6 +343,17 @@ void gather_launch(const T* in, const int* idx, long long off, T* out, long long
 template void gather_launch<double>(const double*, const int*, long long, double*, long long, cudaStream_t);
 template void gather_launch<float>(const float*, const int*, long long, float*, long long, cudaStream_t);
 template void gather_launch<int>(const int*, const int*, long long, int*, long long, cudaStream_t);
+
+long long first_nonfinite(const double* v, long long n) {
+    DevBuf<unsigned long long> first(1);
+    const unsigned long long init = (unsigned long long)n;
+    VG_CUDA(cudaMemcpy(first.data(), &init, sizeof(init), cudaMemcpyHostToDevice));
+    k_first_nonfinite<<<148 * 4, 256>>>(v, n, first.data());
+    VG_CUDA(cudaGetLastError());
+    unsigned long long out = init;
+    VG_CUDA(cudaMemcpy(&out, first.data(), sizeof(out), cudaMemcpyDeviceToHost));
+    return out < init ? (long long)out : -1;
+}
 
 void axpy64_kernel_launch(double* x, const double* d, double a, long long n, cudaStream_t s) {
     k_axpy64<<<148 * 4, 256, 0, s>>>(x, d, a, n);

@@ -181,6 +181,7 @@ int vg_apply(vg_handle* h, const void* x, void* y, int precision, int constraine
     return guarded(h, [&](vg::Solver& s) {
         if (!s.built) throw vg::Error(VG_ESTATE, "vg_build must run before vg_apply");
         if (!x || !y || x == y) throw vg::Error(VG_EINVAL, "apply requires distinct non-null vectors");
+        s.check_apply_probe();
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         const bool internal = (precision & VG_ORDER_INTERNAL) != 0;
         precision &= ~VG_ORDER_INTERNAL;
@@ -201,6 +202,14 @@ int vg_apply(vg_handle* h, const void* x, void* y, int precision, int constraine
         } else {
             throw vg::Error(VG_EINVAL, "precision must be VG_FP64 or VG_FP32");
         }
+        s.probe_apply_error(st);
+    });
+}
+
+int vg_debug_stall_apply(vg_handle* h) {
+    return guarded(h, [&](vg::Solver& s) {
+        if (!s.built) throw vg::Error(VG_ESTATE, "vg_build must run before vg_debug_stall_apply");
+        s.inject_apply_stall();
     });
 }
 

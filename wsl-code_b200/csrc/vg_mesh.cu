@@ -91,8 +91,15 @@ void process_polygons(HostMesh& m, int nn, const double* xy, int nc, const int* 
         for (int i = 0; i < n; ++i) {
             int a = m.cnodes[ptr[c] + i], b = m.cnodes[ptr[c] + (i + 1) % n];
             if (a < 0 || a >= nn || b < 0 || b >= nn) throw Error(VG_EMESH, "node index out of range");
-            s += m.xy[2 * a] * m.xy[2 * b + 1] - m.xy[2 * b] * m.xy[2 * a + 1];
+            const double xa = m.xy[2 * a], ya = m.xy[2 * a + 1], xb = m.xy[2 * b], yb = m.xy[2 * b + 1];
+            if (!std::isfinite(xa) || !std::isfinite(ya))
+                throw Error(VG_EMESH, "cell " + std::to_string(c) + " has a non-finite node coordinate");
+            if (a == b || (xa == xb && ya == yb))
+                throw Error(VG_EMESH, "cell " + std::to_string(c) + " has a zero-length edge");
+            s += xa * yb - xb * ya;
         }
+        // the reference rejects cells without positive size (vem/CurvedVEM_Darcy_gpu/src/mesh_pack.cpp:77-78)
+        if (!(std::fabs(s) > 0)) throw Error(VG_EMESH, "degenerate element: cell " + std::to_string(c) + " has zero area");
         if (s < 0) std::reverse(m.cnodes.begin() + ptr[c], m.cnodes.begin() + ptr[c + 1]);
     }
     m.cx.assign(nc, 0);

@@ -32,6 +32,7 @@ void schur_values(const int* sptr, const int* scol, int nrows, int q, int k, con
 void contract_adjoint(const double* A, const int* map, const int* slot_cell, const int* mask, const Piece* pieces,
                       int npieces, int k, const double* x, const double* mu, int constrained, double* g,
                       cudaStream_t s);
+long long first_nonfinite(const double* v, long long n);
 
 namespace {
 
@@ -287,6 +288,13 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
 Solver::~Solver() {
     destroy_graphs();
     ms_destroy_graphs();
+    if (probe_) {
+        cudaStreamSynchronize(probe_);
+        cudaStreamDestroy(probe_);
+    }
+    if (ev_applied_) cudaEventDestroy(ev_applied_);
+    if (ev_probed_) cudaEventDestroy(ev_probed_);
+    if (h_err_) cudaFreeHost(h_err_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (ev_in_) cudaEventDestroy(ev_in_);
@@ -445,6 +453,17 @@ void Solver::set_problem(int problem_, int bc_) {
 
 void Solver::set_theta(const double* theta, bool on_device) {
     if (!theta) throw Error(VG_EINVAL, "null theta");
+    // a non-finite log permeability would turn the operator and every solve into NaN: rejected
+    // before the handle's field changes
+    long long bad = -1;
+    if (on_device) {
+        VG_CUDA(cudaDeviceSynchronize());  // theta may come from any stream
+        bad = first_nonfinite(theta, m.nc);
+    } else {
+        for (int c = 0; c < m.nc && bad < 0; ++c)
+            if (!std::isfinite(theta[c])) bad = c;
+    }
+    if (bad >= 0) throw Error(VG_EINVAL, "non-finite log permeability in cell " + std::to_string(bad));
     if (on_device)
         VG_CUDA(cudaMemcpy(d_theta_.data(), theta, sizeof(double) * m.nc, cudaMemcpyDeviceToDevice));
     else
@@ -881,6 +900,9 @@ void Solver::plan_streams() {
     d_cta32_.upload(plan32_.cta_batch);
     d_err_.resize(1);
     d_err_.zero();
+    d_stall_.resize(1);
+    d_stall_.zero();
+    VG_CUDA(cudaDeviceSynchronize());
     prepare_stream_kernels();
 }
 
@@ -894,6 +916,49 @@ void Solver::pack_streams(cudaStream_t s) {
     VG_CUDA(cudaStreamSynchronize(s));
 }
 
+// Test hook of the failure path: the next streamed apply leaves one batch uncopied, so that the
+// consumers' bounded waits run out and the apply reports its error word.
+void Solver::inject_apply_stall() {
+    if (k > 1 || !d_stall_.data()) throw Error(VG_ESTATE, "no streamed apply on this handle (k > 1)");
+    const int one = 1;
+    VG_CUDA(cudaMemcpy(d_stall_.data(), &one, sizeof(one), cudaMemcpyHostToDevice));
+}
+
+// vg_apply is asynchronous: after its kernel, a copy of the error word is queued on a private
+// stream (ordered after the caller's stream by an event) into pinned host memory. The next call
+// on the handle looks at the copy if it has completed and reports a failed apply as VG_ECUDA;
+// the caller's stream never waits for it.
+void Solver::probe_apply_error(cudaStream_t s) {
+    if (k > 1 || !d_err_.data()) return;
+    if (!probe_) {
+        VG_CUDA(cudaStreamCreateWithFlags(&probe_, cudaStreamNonBlocking));
+        VG_CUDA(cudaEventCreateWithFlags(&ev_applied_, cudaEventDisableTiming));
+        VG_CUDA(cudaEventCreateWithFlags(&ev_probed_, cudaEventDisableTiming));
+        VG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h_err_), sizeof(int), cudaHostAllocDefault));
+        *h_err_ = 0;
+    }
+    VG_CUDA(cudaEventRecord(ev_applied_, s));
+    VG_CUDA(cudaStreamWaitEvent(probe_, ev_applied_, 0));
+    VG_CUDA(cudaMemcpyAsync(h_err_, d_err_.data(), sizeof(int), cudaMemcpyDeviceToHost, probe_));
+    VG_CUDA(cudaEventRecord(ev_probed_, probe_));
+    probe_pending_ = true;
+}
+
+void Solver::check_apply_probe() {
+    if (!probe_pending_) return;
+    const cudaError_t q = cudaEventQuery(ev_probed_);
+    if (q == cudaErrorNotReady) return;
+    VG_CUDA(q);
+    probe_pending_ = false;
+    if (*h_err_) {
+        *h_err_ = 0;
+        VG_CUDA(cudaDeviceSynchronize());
+        d_err_.zero();
+        VG_CUDA(cudaDeviceSynchronize());
+        throw Error(VG_ECUDA, "an earlier vg_apply failed: apply pipeline wait timed out");
+    }
+}
+
 // the bulk-copy apply sets the error word when a pipeline wait gave up (never in a correct run)
 void Solver::check_pipeline() {
     if (amg_.ready() && amg_.failed()) throw Error(VG_ECUDA, "multigrid copy wait timed out");
@@ -903,6 +968,11 @@ void Solver::check_pipeline() {
     if (e) {
         d_err_.zero();
         VG_CUDA(cudaDeviceSynchronize());
+        if (probe_pending_) {  // the same failure is not reported twice
+            VG_CUDA(cudaStreamSynchronize(probe_));
+            *h_err_ = 0;
+            probe_pending_ = false;
+        }
         throw Error(VG_ECUDA, "apply pipeline wait timed out");
     }
 }
@@ -961,6 +1031,7 @@ ApplyArgs<T> Solver::apply_args(const T* x, T* y, bool constrained, T psign, dou
         a.stages = pl.stages;
         a.stage_bytes = pl.stage_bytes;
         a.err = d_err_.data();
+        a.stall = d_stall_.data();
     }
     return a;
 }

@@ -85,6 +85,7 @@ def lib():
         L.vg_ms_apply.argtypes = [P, P, P, P, I]
         L.vg_ms_step.argtypes = [P, P, P, ctypes.POINTER(VgSolveOpts), ctypes.POINTER(VgSolveInfo)]
         L.vg_stats.argtypes = [P, P]
+        L.vg_debug_stall_apply.argtypes = [P]
         _lib = L
     return _lib
 
