@@ -29,6 +29,7 @@ for p in (os.path.join(ROOT, "wsl-code_b200"), os.path.join(ROOT, "oracle")):
 METRIC = "Darcy solve s @1e-10 vs FP64 oracle: FP32-refined vs FP64 GPU; HBM GB/s; grad/solve"
 CACHE = os.path.join(ROOT, "wsl-code_b200", "_meshcache")
 INNER_TOL = 1e-6  # FP32 inner MINRES: relative reduction per refinement step
+PARITY_TOL = 1e-12  # residual of the solves compared with the oracle
 
 
 def parse():
@@ -163,39 +164,170 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def cpu_reference(args, threads):
-    """The reference CPU algorithm restated (oracle): assembly + GMRES(100)+ILU(0), one sample solve."""
+def cpu_info():
+    """Host CPU model and logical core count (the CPU legs run on this host)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "logical_cores": os.cpu_count() or 1}
+
+
+def _load_by_path(name, path):
+    """A module loaded from its file alone (no package __init__, so no library is mapped)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_sample(args):
+    """Mesh and log permeability of the CPU reference runs: the oracle's own scipy Voronoi + Lloyd
+    annulus (oracle/meshgen_ref.py) and the same Gaussian random field generator as the GPU
+    workload (sigma 2, correlation length 0.1), for the bounded sample size."""
+    import meshgen_ref
+    fields = _load_by_path("vg_fields", os.path.join(ROOT, "wsl-code_b200", "vemgpu", "fields.py"))
+    mesh = meshgen_ref.voronoi_mesh(args.cpu_sample_cells, "annulus", seed=args.seed)
+    theta = fields.gaussian_field(fields.cell_centroids(mesh), sigma=2.0, corr=0.1, seed=args.seed + 1)
+    return mesh, theta
+
+
+def cpu_solve(mesh, theta, threads, problem=None):
+    """The reference CPU algorithm restated in the oracle: element matrices, CSR assembly (OpenMP
+    over `threads` cores) and GMRES(100) + ILU(0) to rtol 1e-10 (one core, like PETSc on
+    PETSC_COMM_SELF). Returns (x, iterations, times)."""
     import oracle as O
-    mesh, theta = annulus_problem(args.cpu_sample_cells, args.seed)
-    x, it, tm = O.reference_solve(mesh, k=0, nq=9, ng=9, geom=O.GEOM_ARCS, problem=O.PROB_ANNULUS,
-                                  bc=O.BC_PRESSURE, theta=theta, threads=threads, rtol=1e-10, maxit=200000)
-    return tm["assembly_s"] + tm["solve_s"], it, tm
+    return O.reference_solve(mesh, k=0, nq=9, ng=9, geom=O.GEOM_ARCS, problem=problem or O.PROB_ANNULUS,
+                             bc=O.BC_PRESSURE, theta=theta, threads=threads, rtol=1e-10, maxit=2000000)
 
 
 def reference_arm(args, rank):
+    """The reference's CPU path for this workload, measured: every step is one full CPU solve
+    (assembly + GMRES(100)+ILU(0), rtol 1e-10) of a bounded sample of the workload, the
+    annulus family at --cpu-sample-cells cells. `value` is the measured seconds per sample solve
+    on the sample's own cell count; the 1M-cell workload itself takes hours on one core and is
+    not run (a linear lower-bound estimate is reported beside the value, labelled as such)."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    times = []
+    mesh, theta = reference_sample(args)
+    cells = len(mesh["cell_ptr"]) - 1
+    times, asm, sol = [], [], []
     for i in range(args.warmup + args.steps):
-        t, it, tm = cpu_reference(args, threads)
+        _, it, tm = cpu_solve(mesh, theta, threads)
         if i >= args.warmup:
-            times.append(t)
-    sample = sum(times) / len(times)
-    value = sample * args.cells / args.cpu_sample_cells
+            times.append(tm["assembly_s"] + tm["solve_s"])
+            asm.append(tm["assembly_s"])
+            sol.append(tm["solve_s"])
+    value = sum(times) / len(times)
+    cpu = cpu_info()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"annulus {args.cells} Voronoi cells, k=0, lognormal K, Dirichlet p=1/0",
-                       "sample_cells": args.cpu_sample_cells},
+            "config": {"workload": f"annulus 0.3<r<1, {cells} Voronoi+Lloyd cells (exact arcs), k=0, lognormal K "
+                                   f"(sigma 2, corr 0.1), p=1 inner / 0 outer, to ||b-Ax||/||b|| <= 1e-10: a bounded "
+                                   f"sample of the {args.cells}-cell workload",
+                       "cells": cells, "sample_of_cells": args.cells, "k": 0, "nq": 9, "ng": 9,
+                       "parallelism": "CPU: assembly on all cores, GMRES+ILU(0) on one"},
+            "cpu": cpu, "assembly_s": sum(asm) / len(asm), "gmres_ilu_s": sum(sol) / len(sol), "iterations": it,
+            "estimate_full_workload_s": {"value": value * args.cells / cells, "kind": "estimate, not measured: "
+                                         "linear in cells, a lower bound (GMRES+ILU iterations grow with the mesh)"},
             "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
                              "sample": f"reference algorithm restated (oracle): element matrices + CSR assembly "
-                                       f"({threads} threads) + GMRES(100)+ILU(0) rtol 1e-10 (1 thread) on a "
-                                       f"{args.cpu_sample_cells}-cell annulus of the same family, {sample:.2f} s per "
-                                       f"solve, {it} iterations, scaled linearly to {args.cells} cells (a lower "
-                                       f"bound: iterations grow with size)"},
+                                       f"({threads} threads) + GMRES(100)+ILU(0) rtol 1e-10 (1 thread) on a {cells}-cell "
+                                       f"annulus of the same family (oracle mesh generator), measured per solve, "
+                                       f"{it} iterations; CPU {cpu['model']}"},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def _oracle_worker(kind, mesh_path, theta, conn):
+    """Spawned child process: the oracle's CPU FP64 checks on the 250k-cell meshes (numpy, scipy
+    and the oracle library only; no CUDA). Runs beside the GPU legs; talks through `conn`.
+
+    kind "c2": the disk problem (p = sin(pi x) sin(pi y), K = I, Dirichlet pressure), k = 0 by
+    sparse LU (the golden discrete solution) with its six error figures; then, for the k = 1 GPU
+    solution it receives, the oracle's own residual ||b - K x|| / ||b|| and error figures (a sparse
+    LU of the 3M-unknown k = 1 system exceeds SuperLU's limits here).
+    kind "c4": the annulus with log permeability theta: one sparse LU gives the forward solution;
+    for the observation rows and data it receives, J, dJ/dx, the adjoint lam = K^-T dJ/dx and the
+    per-cell gradient lam_E^T A_E x_E (the CPU FP64 gradient)."""
+    import numpy as np
+    import scipy.sparse.linalg as spla
+    import oracle as O
+    try:
+        z = np.load(mesh_path)
+        mesh = {k: z[k] for k in z.files}
+        t0 = time.time()
+        if kind == "c2":
+            o = O.Oracle(mesh, k=0, nq=9, ng=9, geom=O.GEOM_ARCS, problem=O.PROB_SINSIN, bc=O.BC_PRESSURE, threads=4)
+            xo, _, _ = o.solve_direct()
+            conn.send({"x": xo, "seconds": time.time() - t0, "errors": o.errors(xo), "N": o.N})
+            del o
+            x1 = conn.recv()
+            if x1 is not None:
+                o1 = O.Oracle(mesh, k=1, nq=9, ng=9, geom=O.GEOM_ARCS, problem=O.PROB_SINSIN, bc=O.BC_PRESSURE,
+                              threads=4)
+                K1, b1 = o1.system()
+                r = float(np.linalg.norm(b1 - K1 @ x1) / np.linalg.norm(b1))
+                conn.send({"residual": r, "errors": o1.errors(x1), "N": o1.N})
+        else:
+            o = O.Oracle(mesh, k=0, nq=9, ng=9, geom=O.GEOM_ARCS, problem=O.PROB_ANNULUS, bc=O.BC_PRESSURE,
+                         theta=theta, threads=4)
+            K, b = o.system()
+            lu = spla.splu(K.tocsc(), permc_spec="COLAMD")
+            x = lu.solve(b)
+            t_lu = time.time() - t0
+            req = conn.recv()
+            if req is not None:
+                idx, data = req
+                r = x[idx] - data
+                dJdx = np.zeros(o.N)
+                np.add.at(dJdx, idx, 2.0 * r)
+                lam = lu.solve(dJdx, trans="T")
+                g = o.adjoint_contract(x, lam)
+                conn.send({"J": float(r @ r), "g": g, "x_obs": x[idx], "seconds": t_lu, "N": o.N})
+    except Exception as e:  # reported by the parent, never silently dropped
+        conn.send({"error": f"{type(e).__name__}: {e}"})
+    finally:
+        conn.close()
+
+
+class OracleJob:
+    """One spawned oracle check (spawn context: no state of the parent's CUDA context)."""
+
+    def __init__(self, kind, mesh_path, theta=None):
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        self.conn, child = ctx.Pipe()
+        self.p = ctx.Process(target=_oracle_worker, args=(kind, mesh_path, theta, child), daemon=True)
+        self.p.start()
+        child.close()
+
+    def send(self, obj):
+        self.conn.send(obj)
+
+    def recv(self, timeout=1800):
+        if not self.conn.poll(timeout):
+            raise RuntimeError("oracle check did not answer in time")
+        out = self.conn.recv()
+        if isinstance(out, dict) and "error" in out:
+            raise RuntimeError("oracle check failed: " + out["error"])
+        return out
+
+    def close(self):
+        try:
+            self.conn.close()
+        finally:
+            self.p.join(timeout=60)
+            if self.p.is_alive():
+                self.p.terminate()
 
 
 def adjoint_leg(args, rank):
@@ -316,13 +448,99 @@ def ms_leg(args):
     return out
 
 
-def config1_leg(args):
-    """Disk problem of the reference's own examples at 250k cells: p = sin(pi x) sin(pi y), Dirichlet
-    pressure, K = I, k = 0 and k = 1, FP64 and mixed solves to 1e-10 (device time) and the L2 errors
-    against the manufactured solution."""
+def same_size_leg(args):
+    """CPU reference algorithm and GPU solver on the same mesh: the --cpu-sample-cells annulus of
+    the workload's family (same generator, seed and log-permeability field as the workload). CPU:
+    assembly on one core and on all cores, GMRES(100)+ILU(0) to 1e-10 on one core, measured. GPU:
+    handle set-up (mesh processing, device set-up kernels, multigrid) by wall clock, FP64 and mixed
+    solves to 1e-10 by device time, and the end-to-end host-buffer solve."""
+    import vemgpu
+    mesh, _ = annulus_problem(args.cpu_sample_cells, args.seed)
+    from vemgpu import fields
+    theta = fields.gaussian_field(fields.cell_centroids(mesh), sigma=2.0, corr=0.1, seed=replica_seed(args.seed, 0))
+    cells = len(mesh["cell_ptr"]) - 1
+    out = {"cells": cells, "cpu": cpu_info()}
+    for name, threads in (("cpu_1core", 1), ("cpu_allcore", os.cpu_count() or 1)):
+        _, it, tm = cpu_solve(mesh, theta, threads)
+        out[name] = {"assembly_s": tm["assembly_s"], "gmres_ilu_s": tm["solve_s"], "iterations": it,
+                     "assembly_threads": threads}
+    t0 = time.time()
+    g = vemgpu.DarcyGpu(mesh, k=0, nq=9, ng=9, geometry="arcs", problem="annulus", bc="pressure", theta=theta)
+    b = g.rhs()
+    import torch
+    torch.cuda.synchronize()
+    out["gpu_setup_s"] = time.time() - t0
+    for mode in ("fp64", "mixed"):
+        g.solve(b, mode=mode, tol=1e-10, inner_tol=INNER_TOL)
+        ts = [g.solve(b, mode=mode, tol=1e-10, inner_tol=INNER_TOL)[1]["seconds"] for _ in range(5)]
+        out[f"gpu_{mode}_solve_s"] = sum(ts) / len(ts)
+    bh = b.cpu().numpy()
+    g.solve_host(bh, mode="mixed", tol=1e-10, inner_tol=INNER_TOL)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        g.solve_host(bh, mode="mixed", tol=1e-10, inner_tol=INNER_TOL)
+    out["gpu_mixed_e2e_s"] = (time.perf_counter() - t0) / 5
+    g.close()
+    c1 = out["cpu_1core"]
+    out["ratio_solve_vs_mixed"] = c1["gmres_ilu_s"] / out["gpu_mixed_solve_s"]
+    out["ratio_solve_vs_fp64"] = c1["gmres_ilu_s"] / out["gpu_fp64_solve_s"]
+    out["ratio_e2e"] = (c1["assembly_s"] + c1["gmres_ilu_s"]) / out["gpu_mixed_e2e_s"]
+    out["ratio_setup_plus_solve"] = (out["cpu_allcore"]["assembly_s"] + out["cpu_allcore"]["gmres_ilu_s"]) / (
+        out["gpu_setup_s"] + out["gpu_mixed_solve_s"])
+    return out
+
+
+def c1_leg(args):
+    """Config C1: the 1,000-cell Voronoi disk, k = 0, K = I, p = sin(pi x) sin(pi y), Dirichlet
+    pressure. CPU: the reference algorithm restated in the oracle (assembly + GMRES(100)+ILU(0),
+    rtol 1e-10, one core), timed, with its flux and pressure L2 errors (the figures the reference
+    prints per run, vem/CurvedVEM_Darcy/main/Darcy_curved_main.cpp:84-92) and the oracle's sparse-LU
+    solution; GPU: FP64 and mixed solves to PARITY_TOL with the same figures and their relative
+    distance to the LU solution."""
+    import numpy as np
+    import oracle as O
+    import vemgpu
+    mesh = disk_mesh(1000, args.seed)
+    o = O.Oracle(mesh, k=0, nq=9, ng=9, geom=O.GEOM_ARCS, problem=O.PROB_SINSIN, bc=O.BC_PRESSURE)
+    xo, _, _ = o.solve_direct()
+    e_lu = o.errors(xo)
+    xr, it, tm = cpu_solve(mesh, None, 1, problem=O.PROB_SINSIN)
+    e_cpu = o.errors(xr)
+    out = {"cells": o.nc, "dofs": o.N,
+           "cpu_reference": {"seconds": tm["assembly_s"] + tm["solve_s"], "iterations": it, "residual": tm["rel"],
+                             "l2_pressure": e_cpu["scalar_comp"], "l2_flux": e_cpu["flux_comp"],
+                             "l2_pressure_phys": e_cpu["scalar_phys"], "l2_flux_phys": e_cpu["flux_phys"],
+                             "rel_err_vs_lu": float(np.linalg.norm(xr - xo) / np.linalg.norm(xo))},
+           "oracle_lu": {"l2_pressure": e_lu["scalar_comp"], "l2_flux": e_lu["flux_comp"]}}
+    g = vemgpu.DarcyGpu(mesh, k=0, geometry="arcs", problem="sinsin", bc="pressure")
+    for mode in ("fp64", "mixed"):
+        g.solve(tol=PARITY_TOL, mode=mode, inner_tol=INNER_TOL)
+        x, info = g.solve(tol=PARITY_TOL, mode=mode, inner_tol=INNER_TOL)
+        e = g.errors(x)
+        xg = x.cpu().numpy()
+        out[mode] = {"solve_s": info["seconds"], "iterations": info["iterations"], "residual": info["residual"],
+                     "rel_err_vs_lu": float(np.linalg.norm(xg - xo) / np.linalg.norm(xo)),
+                     "l2_pressure": e["scalar_comp"], "l2_flux": e["flux_comp"]}
+    g.close()
+    return out
+
+
+def c2_leg(args, job):
+    """Config C2: the 250,000-cell disk of C1's problem, k = 0 and k = 1, FP64 and mixed solves to
+    relative residual 1e-10 (device time) with the L2 errors against the manufactured solution,
+    and the solves to PARITY_TOL compared with the oracle: for k = 0 the relative distance to the
+    oracle's sparse-LU solution, for k = 1 the oracle's own residual ||b - K x|| / ||b|| of the GPU
+    solution (the spawned check `job`, which ran beside the GPU legs)."""
+    import numpy as np
     import vemgpu
     mesh = disk_mesh(args.config1_cells, args.seed)
     out = {"cells": len(mesh["cell_ptr"]) - 1}
+    xo = None
+    if job is not None:
+        r = job.recv()
+        xo = r["x"]
+        out["oracle_lu_k0"] = {"seconds": r["seconds"], "l2_pressure": r["errors"]["scalar_comp"],
+                               "l2_flux": r["errors"]["flux_comp"]}
     for k in (0, 1):
         g = vemgpu.DarcyGpu(mesh, k=k, geometry="arcs", problem="sinsin", bc="pressure")
         row = {"dofs": g.N}
@@ -330,10 +548,24 @@ def config1_leg(args):
             g.solve(tol=1e-10, mode=mode, inner_tol=INNER_TOL)
             x, info = g.solve(tol=1e-10, mode=mode, inner_tol=INNER_TOL)
             row[mode] = {"solve_s": info["seconds"], "iterations": info["iterations"], "residual": info["residual"]}
+            xp, infop = g.solve(tol=PARITY_TOL, mode=mode, inner_tol=INNER_TOL)
+            row[mode].update(parity_solve_s=infop["seconds"], parity_residual=infop["residual"])
+            if k == 0 and xo is not None:
+                xg = xp.cpu().numpy()
+                row[mode]["rel_err_vs_oracle_lu"] = float(np.linalg.norm(xg - xo) / np.linalg.norm(xo))
+                row[mode]["rel_err_vs_oracle_lu_at_1e-10"] = float(np.linalg.norm(x.cpu().numpy() - xo) /
+                                                                   np.linalg.norm(xo))
         e = g.errors(x)
         row["l2_pressure"], row["l2_flux"] = e["scalar_phys"], e["flux_phys"]
+        if k == 1 and job is not None:
+            job.send(xp.cpu().numpy())
+            r = job.recv()
+            row["oracle_residual_of_gpu_solution"] = r["residual"]
+            row["oracle_vs_gpu_l2_pressure"] = abs(r["errors"]["scalar_phys"] / e["scalar_phys"] - 1)
         out[f"k{k}"] = row
         g.close()
+    if job is not None:
+        job.close()
     return out
 
 
@@ -491,16 +723,19 @@ def ours(args, rank, world, dist):
             e2e.append(time.perf_counter() - t)
     e2e_s = max_over_ranks(sum(e2e) / len(e2e), dist)
     adjoint = None if args.no_adjoint else adjoint_leg(args, rank)
-    config1 = None if args.no_config1 else config1_leg(args)
+    config1 = None if args.no_config1 else c2_leg(args, None)
+    c1 = None if args.no_config1 else c1_leg(args)
     ms = None if args.no_ms else ms_leg(args)
-    cpu = None
+    cpu = same = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
-        threads = 1
-        tcpu, it, tm = cpu_reference(args, threads)
-        cpu = {"value": tcpu * args.cells / args.cpu_sample_cells, "unit": "s", "cores": threads, "kind": "port",
+        same = same_size_leg(args)
+        one = same["cpu_1core"]
+        cpu = {"value": one["assembly_s"] + one["gmres_ilu_s"], "unit": "s", "cores": 1, "kind": "port",
+               "cells": same["cells"],
                "sample": f"reference algorithm restated (oracle): element matrices, CSR assembly, GMRES(100)+ILU(0) "
-                         f"rtol 1e-10 on a {args.cpu_sample_cells}-cell annulus of the same family, one core: "
-                         f"{tcpu:.2f} s ({it} iterations), scaled linearly to {args.cells} cells (lower bound)"}
+                         f"rtol 1e-10 on one core, measured per solve on a {same['cells']}-cell annulus of the "
+                         f"workload's family (not scaled; the same mesh solved on the GPU in same_size: "
+                         f"{same['ratio_solve_vs_mixed']:.0f}x); CPU {same['cpu']['model']}"}
     if rank != 0:
         return
     contrast = float(np.exp(theta.max() - theta.min()))
@@ -532,9 +767,11 @@ def ours(args, rank, world, dist):
         "assembled_comparator": assembled,
         "adjoint": adjoint,
         "disk_250k": config1,
+        "disk_1k": c1,
         "maxwell_stefan": ms,
         "gpu_launches": launches,
         "clocks": clocks,
+        "same_size": same,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)

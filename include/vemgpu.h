@@ -227,9 +227,18 @@ int vg_ms_configure(vg_handle* h, double d12, double d13, double d23, double dt,
 /* y = K(coeff_state) x for the Maxwell-Stefan system (FP64 or FP32 x, y; device). */
 int vg_ms_apply(vg_handle* h, const double* coeff_state, const void* x, void* y, int precision);
 /* One backward-Euler step: solve K(old) new = [0; |E|/dt x_old] to ||b - K new|| / ||b|| <= opts->tol
- * by right-preconditioned GMRES(10), FP64 or FP32 inner under FP64 refinement (opts->mode). */
+ * by right-preconditioned GMRES(10), FP64 or FP32 inner under FP64 refinement (opts->mode). With
+ * Picard iterations enabled (vg_ms_set_picard), the friction matrix is re-evaluated at the latest
+ * iterate and the system solved again until the step is fully implicit to the Picard tolerance. */
 int vg_ms_step(vg_handle* h, const double* old_state, double* new_state, const vg_solve_opts* opts,
                vg_solve_info* info);
+/* Picard iterations of vg_ms_step (the reference's loop, vem/CurvedVEM_Darcy_gpu/src/solver_driver.cpp:209-240):
+ * max_iterations = 1 (the default) keeps the friction matrix at x^n (linearly implicit step);
+ * > 1 iterates K(x^{n+1,m}) x^{n+1,m+1} = b until ||x^{m+1} - x^m|| / max(1, ||x^{m+1}||) <= tol and
+ * the nonlinear residual ||b - K(x) x|| / ||b|| at the accepted x is <= max(tol, 5 opts->tol);
+ * VG_ENOCONV otherwise. vg_ms_picard_info reports the last step's iterations, change and residual. */
+int vg_ms_set_picard(vg_handle* h, int max_iterations, double tol);
+int vg_ms_picard_info(const vg_handle* h, int* iterations, double* change, double* nonlinear_residual);
 
 /* ---- post-processing ---------------------------------------------------------------------- */
 

@@ -115,3 +115,35 @@ def test_steps_conserve_mass_and_sum(case):
     x64 = torch.cat(ms.fractions(s64)[:2])
     x32 = torch.cat(ms.fractions(s32)[:2])
     assert float(torch.linalg.norm(x64 - x32) / torch.linalg.norm(x64)) <= 1e-9
+
+
+def test_picard_step_matches_cpu_picard(case):
+    """Fully implicit step: Picard iterations on the friction matrix (the reference's time loop,
+    vem/CurvedVEM_Darcy_gpu/src/solver_driver.cpp:209-240) against the same iteration on the CPU
+    system, each linear system by sparse LU; relative 1e-9 between the two fixed points."""
+    m, o, _, x1, x2 = case
+    ms = MaxwellStefan(m, D=D, dt=DT, picard=20, picard_tol=1e-11)
+    s = ms.state(x1, x2)
+    areas = np.array([o.local(c, "L")[0] for c in range(o.nc)])
+    b = np.zeros(ms.N)
+    b[2 * o.nf:] = np.r_[areas * x1, areas * x2] / DT
+    xk = s.cpu().numpy()
+    for it in range(20):
+        nxt = xk[2 * o.nf:]
+        xn = spla.spsolve(cpu_system(o, nxt[:o.nc], nxt[o.nc:]).tocsc(), b)
+        change = np.linalg.norm(xn - xk) / max(1.0, np.linalg.norm(xn))
+        xk = xn
+        if change <= 1e-13:
+            break
+    for mode in ("fp64", "mixed"):
+        new, info = ms.step(s, mode=mode, tol=1e-12)
+        assert info["picard"] >= 2 and info["picard_change"] <= 1e-11 and info["nonlinear_residual"] <= 1e-11
+        got = new.cpu().numpy()
+        assert np.linalg.norm(got - xk) <= 1e-9 * np.linalg.norm(xk), mode
+        # the fully implicit step differs from the linearly implicit one
+        ms.set_picard(1)
+        lin, info1 = ms.step(s, mode=mode, tol=1e-12)
+        assert info1["picard"] == 1
+        assert np.linalg.norm(lin.cpu().numpy() - xk) > 1e-9 * np.linalg.norm(xk)
+        ms.set_picard(20, 1e-11)
+    ms.close()

@@ -351,6 +351,18 @@ int vg_ms_step(vg_handle* h, const double* old_state, double* new_state, const v
     });
 }
 
+int vg_ms_set_picard(vg_handle* h, int max_iterations, double tol) {
+    return guarded(h, [&](vg::Solver& s) { s.ms_set_picard(max_iterations, tol); });
+}
+
+int vg_ms_picard_info(const vg_handle* h, int* iterations, double* change, double* nonlinear_residual) {
+    if (!h || !h->s) return VG_EINVAL;
+    if (iterations) *iterations = h->s->ms_last_picard_;
+    if (change) *change = h->s->ms_last_change_;
+    if (nonlinear_residual) *nonlinear_residual = h->s->ms_last_nonlinear_;
+    return VG_OK;
+}
+
 int vg_local(vg_handle* h, int cell, int which, double* out, int* count) {
     return guarded(h, [&](vg::Solver& s) {
         int c = s.local(cell, which, out);

@@ -887,24 +887,48 @@ void Solver::ms_coefficients(const double* state) {
     VG_CUDA(cudaGetLastError());
 }
 
+void Solver::ms_set_picard(int max_iterations, double tol) {
+    if (max_iterations < 1 || !(tol > 0)) throw Error(VG_EINVAL, "Picard needs max_iterations >= 1 and tol > 0");
+    ms_picard_max_ = max_iterations;
+    ms_picard_tol_ = tol;
+}
+
+// One backward-Euler step. With one Picard iteration (the default) the friction matrix is taken at
+// x^n and one linear system is solved (linearly implicit). With more, the friction matrix is
+// re-evaluated at the latest iterate and the system solved again, until the relative change of
+// the iterate is at most the Picard tolerance and the nonlinear residual ||b - K(x) x|| / ||b||,
+// with K(x) at the accepted state, is at most max(Picard tolerance, 5 linear tolerance): the
+// acceptance of the reference's time loop (vem/CurvedVEM_Darcy_gpu/src/solver_driver.cpp:209-240).
 void Solver::ms_step(const double* old_state, double* new_state, const vg_solve_opts& o, vg_solve_info& info) {
     if (!ms_.ready) throw Error(VG_ESTATE, "vg_ms_configure must run before vg_ms_step");
     if (!(o.tol > 0) || o.maxit < 1 || (o.mode == VG_SOLVE_MIXED && !(o.inner_tol > 0 && o.inner_tol < 1)))
         throw Error(VG_EINVAL, "invalid solve options");
     info = vg_solve_info{};
+    ms_last_picard_ = 0;
+    ms_last_change_ = ms_last_nonlinear_ = 0.0;
     const long long Nm = ms_.N;
+    const int P = ms_picard_max_;
     VG_CUDA(cudaDeviceSynchronize());  // the states may come from any stream
     VG_CUDA(cudaEventRecord(ev0_, stream_));
-    // coefficients and preconditioner at x^n
-    ms_coefficients(old_state);
-    VG_CUDA(cudaMemsetAsync(ms_.D.data(), 0, sizeof(double) * ms_.D.size(), stream_));
-    k_ms_pc_flux<<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS, 0, stream_>>>(
-        d_A0_.data(), d_map_.data(), d_pieces_.data(), int(pieces_.size()), d_slot_cell_.data(), ms_.B64.data(),
-        d_mask_.data(), ms_.D.data());
-    k_ms_pc_flux_inv<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(ms_.D.data(), d_mask_.data(), nf, ms_.F64.data(), ms_.F32.data());
-    k_ms_pc_cell<<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS, 0, stream_>>>(
-        d_map_.data(), d_pieces_.data(), int(pieces_.size()), d_slot_cell_.data(), d_mask_.data(), ms_.F64.data(),
-        ms_.m64.data(), ms_.C64.data(), ms_.C32.data());
+    if (P > 1) {
+        ms_.prev.resize(Nm);
+        VG_CUDA(cudaMemcpyAsync(ms_.prev.data(), old_state, sizeof(double) * Nm, cudaMemcpyDeviceToDevice, stream_));
+    }
+    // friction coefficients and the block preconditioner at a state
+    auto prepare = [&](const double* coeff_state) {
+        ms_coefficients(coeff_state);
+        VG_CUDA(cudaMemsetAsync(ms_.D.data(), 0, sizeof(double) * ms_.D.size(), stream_));
+        k_ms_pc_flux<<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS, 0, stream_>>>(
+            d_A0_.data(), d_map_.data(), d_pieces_.data(), int(pieces_.size()), d_slot_cell_.data(), ms_.B64.data(),
+            d_mask_.data(), ms_.D.data());
+        k_ms_pc_flux_inv<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(ms_.D.data(), d_mask_.data(), nf, ms_.F64.data(),
+                                                                ms_.F32.data());
+        k_ms_pc_cell<<<ms_blocks((long long)pieces_.size() * PIECE), MS_THREADS, 0, stream_>>>(
+            d_map_.data(), d_pieces_.data(), int(pieces_.size()), d_slot_cell_.data(), d_mask_.data(), ms_.F64.data(),
+            ms_.m64.data(), ms_.C64.data(), ms_.C32.data());
+        VG_CUDA(cudaGetLastError());
+    };
+    prepare(old_state);
     if (!ms_.amg_ready) {
         VG_CUDA(cudaStreamSynchronize(stream_));
         try {
@@ -925,27 +949,56 @@ void Solver::ms_step(const double* old_state, double* new_state, const vg_solve_
         if (nb_out) *nb_out = nbv;
         return nr / (nbv > 0 ? nbv : 1.0);
     };
-    double nb = 0;
-    double rel = true_residual(&nb);
     int total = 0, outer = 0;
+    double rel = 0;
+    bool accepted = P == 1;
     const int mres = VG_MS_RESTART;
-    if (o.mode == VG_SOLVE_FP64) {
-        for (outer = 0; outer < 4 && rel > o.tol && total < o.maxit; ++outer) {
-            double r_in = 0;
-            const double rn = rel * nb;
-            total += ms_gmres<double>(ms_.r.data(), ms_.d.data(), std::min(0.5, 0.5 * o.tol * nb / rn), o.maxit - total,
-                                      mres, &r_in);
-            k_axpy_t<double><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(new_state, ms_.d.data(), 1.0, Nm);
-            rel = true_residual(nullptr);
+    for (int pic = 0; pic < P; ++pic) {
+        if (pic > 0) {
+            // the next linear system: friction at the latest iterate, started from it
+            VG_CUDA(cudaMemcpyAsync(ms_.prev.data(), new_state, sizeof(double) * Nm, cudaMemcpyDeviceToDevice,
+                                    stream_));
+            prepare(ms_.prev.data());
         }
-    } else {
-        for (outer = 0; outer < o.max_outer && rel > o.tol && total < o.maxit; ++outer) {
-            const double rn = rel * nb;
-            k_d2f<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(ms_.r.data(), ms_.r32.data(), Nm, 1.0 / rn);
-            double r_in = 0;
-            total += ms_gmres<float>(ms_.r32.data(), ms_.d32.data(), o.inner_tol, o.maxit - total, mres, &r_in);
-            k_addf<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(new_state, ms_.d32.data(), rn, Nm);
-            rel = true_residual(nullptr);
+        double nb = 0;
+        rel = true_residual(&nb);
+        int steps = 0;
+        if (o.mode == VG_SOLVE_FP64) {
+            for (steps = 0; steps < 4 && rel > o.tol && total < o.maxit; ++steps) {
+                double r_in = 0;
+                const double rn = rel * nb;
+                total += ms_gmres<double>(ms_.r.data(), ms_.d.data(), std::min(0.5, 0.5 * o.tol * nb / rn),
+                                          o.maxit - total, mres, &r_in);
+                k_axpy_t<double><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(new_state, ms_.d.data(), 1.0, Nm);
+                rel = true_residual(nullptr);
+            }
+        } else {
+            for (steps = 0; steps < o.max_outer && rel > o.tol && total < o.maxit; ++steps) {
+                const double rn = rel * nb;
+                k_d2f<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(ms_.r.data(), ms_.r32.data(), Nm, 1.0 / rn);
+                double r_in = 0;
+                total += ms_gmres<float>(ms_.r32.data(), ms_.d32.data(), o.inner_tol, o.maxit - total, mres, &r_in);
+                k_addf<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(new_state, ms_.d32.data(), rn, Nm);
+                rel = true_residual(nullptr);
+            }
+        }
+        outer += steps;
+        ms_last_picard_ = pic + 1;
+        if (P == 1) break;
+        if (!(rel <= o.tol)) break;  // the linear solve failed: reported below
+        // relative change of the iterate (the reference's measure: all unknowns, against max(1, |x|))
+        k_sub<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(new_state, ms_.prev.data(), ms_.y.data(), Nm);
+        const double change = ms_norm<double>(ms_.y.data()) / std::max(1.0, ms_norm<double>(new_state));
+        ms_last_change_ = change;
+        if (change <= ms_picard_tol_) {
+            // nonlinear residual with the friction matrix at the accepted state
+            prepare(new_state);
+            const double nonlinear = true_residual(nullptr);
+            ms_last_nonlinear_ = nonlinear;
+            if (nonlinear <= std::max(ms_picard_tol_, 5.0 * o.tol)) {
+                accepted = true;
+                break;
+            }
         }
     }
     VG_CUDA(cudaEventRecord(ev1_, stream_));
@@ -963,6 +1016,9 @@ void Solver::ms_step(const double* old_state, double* new_state, const vg_solve_
     if (!(rel <= o.tol))
         throw Error(VG_ENOCONV, "Maxwell-Stefan step did not converge: iterations=" + std::to_string(total) +
                                     " true_relative_residual=" + std::to_string(rel));
+    if (!accepted)
+        throw Error(VG_ENOCONV, "Maxwell-Stefan Picard iteration did not converge in " + std::to_string(P) +
+                                    " iterations: relative change " + std::to_string(ms_last_change_));
 }
 
 template void Solver::ms_apply<double>(const double*, double*);

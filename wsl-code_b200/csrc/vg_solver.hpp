@@ -67,6 +67,9 @@ public:
     template <typename T>
     void ms_apply(const T* x, T* y);
     long long ms_size() const { return ms_.N; }
+    void ms_set_picard(int max_iterations, double tol);
+    int ms_last_picard_ = 0;
+    double ms_last_change_ = 0, ms_last_nonlinear_ = 0;
     int device() const { return device_; }  // the CUDA device that holds this handle's data
     // failure-path test hook and the asynchronous error report of vg_apply
     void inject_apply_stall();
@@ -131,6 +134,7 @@ private:
         double i12 = 0, i13 = 0, i23 = 0, dt = 0;
         long long N = 0;
         DevBuf<double> B64, F64, C64, D, m64, V64, b, r, y, d, t64, w64, vn64, partials, kry;
+        DevBuf<double> prev;  // Picard: the iterate the friction matrix was taken at
         DevBuf<float> B32, F32, C32, m32, A32, V32, r32, d32, t32, w32, vn32;
         DevBuf<unsigned int> counter;
         long long ld = 0, chunk = 0;  // Krylov basis column stride; rows per dot-product block
@@ -142,7 +146,9 @@ private:
         Amg amg[2];
         bool amg_ready = false;
     } ms_;
-    bool ms_large_ = false;  // pieces of polygons outside 3..9 edges (second apply kernel)
+    bool ms_large_ = false;
+    int ms_picard_max_ = 1;
+    double ms_picard_tol_ = 1e-10;  // pieces of polygons outside 3..9 edges (second apply kernel)
     void ms_build_amg();
     void assembled_pattern();
     std::vector<long long> csr_ptr_;  // assembled pattern (host, built on first request)

@@ -86,6 +86,8 @@ def lib():
         L.vg_ms_step.argtypes = [P, P, P, ctypes.POINTER(VgSolveOpts), ctypes.POINTER(VgSolveInfo)]
         L.vg_stats.argtypes = [P, P]
         L.vg_debug_stall_apply.argtypes = [P]
+        L.vg_ms_set_picard.argtypes = [P, I, D]
+        L.vg_ms_picard_info.argtypes = [P, ctypes.POINTER(I), ctypes.POINTER(D), ctypes.POINTER(D)]
         _lib = L
     return _lib
 

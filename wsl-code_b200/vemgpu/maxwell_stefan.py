@@ -1,8 +1,10 @@
 """Ternary Maxwell-Stefan diffusion on the C ABI (vg_ms_configure / vg_ms_step, k = 0).
 
 State: one device vector [J1, J2, x1, x2] (species fluxes on the flux moments, cell mole fractions),
-x3 = 1 - x1 - x2. Each backward-Euler step solves one coupled two-species saddle-point system with
-the friction matrix frozen at the previous state. The reference's counterpart is its MSGpu time loop
+x3 = 1 - x1 - x2. Each backward-Euler step solves the coupled two-species saddle-point system with
+the friction matrix at the previous state (picard=1, linearly implicit) or, with picard > 1, Picard
+iterations on the friction matrix until the step is fully implicit to picard_tol. The reference's
+counterpart is its MSGpu time loop with Picard iterations
 (vem/CurvedVEM_Darcy_gpu/src/solver_driver.cpp:189-245), which keeps all three species.
 """
 import ctypes
@@ -27,7 +29,8 @@ def initial_fractions(mesh, seed, corr=0.2, lo=0.1, hi=0.8):
 
 
 class MaxwellStefan:
-    def __init__(self, mesh, D=(1.0, 0.5, 0.2), dt=1e-3, geometry="arcs", eps=0.0, device=-1):
+    def __init__(self, mesh, D=(1.0, 0.5, 0.2), dt=1e-3, geometry="arcs", eps=0.0, device=-1, picard=1,
+                 picard_tol=1e-10):
         self.gpu = DarcyGpu(mesh, k=0, geometry=geometry, eps=eps, problem="sincos", bc="flux", device=device)
         self.D, self.dt = tuple(D), dt
         n = ctypes.c_longlong(0)
@@ -37,6 +40,10 @@ class MaxwellStefan:
         torch = _torch()
         self.areas = torch.empty(self.nc, dtype=torch.float64, device="cuda")
         L.check(L.lib().vg_cell_areas(self.gpu.h, self.areas.data_ptr()), self.gpu.h)
+        self.set_picard(picard, picard_tol)
+
+    def set_picard(self, max_iterations, tol=1e-10):
+        L.check(L.lib().vg_ms_set_picard(self.gpu.h, int(max_iterations), float(tol)), self.gpu.h)
 
     def state(self, x1, x2):
         torch = _torch()
@@ -67,7 +74,11 @@ class MaxwellStefan:
         o = DarcyGpu.opts(**kw)
         L.check(L.lib().vg_ms_step(self.gpu.h, s.data_ptr(), out.data_ptr(), ctypes.byref(o), ctypes.byref(info)),
                 self.gpu.h)
-        return out, dict(iterations=info.iterations, outer=info.outer, residual=info.residual, seconds=info.seconds)
+        pic, change, nonlin = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        L.check(L.lib().vg_ms_picard_info(self.gpu.h, ctypes.byref(pic), ctypes.byref(change), ctypes.byref(nonlin)),
+                self.gpu.h)
+        return out, dict(iterations=info.iterations, outer=info.outer, residual=info.residual, seconds=info.seconds,
+                         picard=pic.value, picard_change=change.value, nonlinear_residual=nonlin.value)
 
     def close(self):
         self.gpu.close()
