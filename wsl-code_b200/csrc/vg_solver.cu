@@ -359,8 +359,6 @@ void Solver::internal_copies() {
     d_Lint32_.resize(size_t(np));
     gather_launch<double>(d_L_.data(), d_i2e_.data(), nf, d_Lint_.data(), np, nullptr);
     gather_launch<float>(d_L32_.data(), d_i2e_.data(), nf, d_Lint32_.data(), np, nullptr);
-    for (auto& b : d_pa64_) b.resize(N);
-    for (auto& b : d_pa32_) b.resize(N);
     d_xi_.resize(N);
 }
 
@@ -871,19 +869,59 @@ void Solver::apply_int(const T* x, T* y, bool constrained, T psign, cudaStream_t
 template void Solver::apply_int<double>(const double*, double*, bool, double, cudaStream_t, double*);
 template void Solver::apply_int<float>(const float*, float*, bool, float, cudaStream_t, double*);
 
-// reference order in and out: permute to the internal order, apply, permute back
+// Reference order in and out, in one kernel: the same apply with the dof map, the pressure rows,
+// the essential-BC mask and the multiplier vector in the reference's numbering, and (k <= 1) record
+// streams packed with that map, built on the first call. The gathers and scatters are less
+// coalesced than in the internal order, but no permutation pass runs.
+void Solver::prepare_reference_order() {
+    if (!d_prow_ref_.data()) {
+        std::vector<int> prow(slot_cell_.size(), -1);
+        for (size_t j = 0; j < slot_cell_.size(); ++j)
+            if (slot_cell_[j] >= 0) prow[j] = nf + slot_cell_[j] * q;
+        d_prow_ref_.upload(prow);
+    }
+    if (k <= 1 && !ref_streams_packed_) {
+        d_rec64r_.resize(size_t(plan64_.bytes));
+        d_rec32r_.resize(size_t(plan32_.bytes));
+        pack_streams_reference(nullptr);
+    }
+}
+
+void Solver::pack_streams_reference(cudaStream_t s) {
+    const int np_ = int(pieces_.size());
+    pack_stream<double>(d_pieces_.data(), np_, d_roff64_.data(), d_A64_.data(), d_W64_.data(), d_map_.data(),
+                        d_prow_ref_.data(), k, d_rec64r_.data(), s);
+    pack_stream<float>(d_pieces_.data(), np_, d_roff32_.data(), d_A32_.data(), d_W32_.data(), d_map_.data(),
+                       d_prow_ref_.data(), k, d_rec32r_.data(), s);
+    VG_CUDA(cudaStreamSynchronize(s));
+    ref_streams_packed_ = true;
+}
+
+template <typename T>
+void Solver::apply_ref(const T* x, T* y, bool constrained, T psign, cudaStream_t s, double* quad) {
+    prepare_reference_order();
+    ApplyArgs<T> a = apply_args<T>(x, y, constrained, psign, quad, nullptr);
+    a.map = d_map_.data();
+    a.prow = d_prow_ref_.data();
+    a.mask = d_mask_.data();
+    if constexpr (sizeof(T) == 8) {
+        a.L = d_L_.data();
+        if (a.rec) a.rec = d_rec64r_.data();
+    } else {
+        a.L = d_L32_.data();
+        if (a.rec) a.rec = d_rec32r_.data();
+    }
+    launch_apply(a, s);
+    n_launch += 1;
+    ++n_apply;
+}
+
 void Solver::apply64(const double* x, double* y, bool constrained, double psign, cudaStream_t s, double* quad) {
-    permute<double>(x, d_pa64_[0].data(), true, s);
-    VG_CUDA(cudaMemsetAsync(d_pa64_[1].data(), 0, sizeof(double) * N, s));
-    apply_int<double>(d_pa64_[0].data(), d_pa64_[1].data(), constrained, psign, s, quad);
-    permute<double>(d_pa64_[1].data(), y, false, s);
+    apply_ref<double>(x, y, constrained, psign, s, quad);
 }
 
 void Solver::apply32(const float* x, float* y, bool constrained, float psign, cudaStream_t s, double* quad) {
-    permute<float>(x, d_pa32_[0].data(), true, s);
-    VG_CUDA(cudaMemsetAsync(d_pa32_[1].data(), 0, sizeof(float) * N, s));
-    apply_int<float>(d_pa32_[0].data(), d_pa32_[1].data(), constrained, psign, s, quad);
-    permute<float>(d_pa32_[1].data(), y, false, s);
+    apply_ref<float>(x, y, constrained, psign, s, quad);
 }
 
 void Solver::plan_streams() {
@@ -914,6 +952,7 @@ void Solver::pack_streams(cudaStream_t s) {
     pack_stream<float>(d_pieces_.data(), np_, d_roff32_.data(), d_A32_.data(), d_W32_.data(), d_map_int_.data(),
                        d_prow_.data(), k, d_rec32_.data(), s);
     VG_CUDA(cudaStreamSynchronize(s));
+    if (ref_streams_packed_) pack_streams_reference(s);  // new operator values (permeability update)
 }
 
 // Test hook of the failure path: the next streamed apply leaves one batch uncopied, so that the

@@ -105,6 +105,13 @@ public:
 private:
     void plan_streams();
     void pack_streams(cudaStream_t s);
+    void prepare_reference_order();
+    void pack_streams_reference(cudaStream_t s);
+    template <typename T>
+    void apply_ref(const T* x, T* y, bool constrained, T psign, cudaStream_t s, double* quad);
+    DevBuf<int> d_prow_ref_;                // per slot: first pressure row in the reference order
+    DevBuf<unsigned char> d_rec64r_, d_rec32r_;  // record streams with the reference-order map
+    bool ref_streams_packed_ = false;
     void check_pipeline();
     void make_diagonal(cudaStream_t s);
     void lift_flux_rhs();
@@ -235,8 +242,8 @@ private:
     // the public entry points keep the reference's order and permute at the boundary
     std::vector<int> map_int_host_, prow_host_, e2i_host_, i2e_host_;
     DevBuf<int> d_map_int_, d_prow_, d_e2i_, d_i2e_, d_mask_int_;
-    DevBuf<double> d_Lint_, d_pdinv64_, d_pa64_[2], d_xi_;
-    DevBuf<float> d_Lint32_, d_pdinv32_, d_pa32_[2];
+    DevBuf<double> d_Lint_, d_pdinv64_, d_xi_;
+    DevBuf<float> d_Lint32_, d_pdinv32_;
 public:
     // x (N) to or from the internal order
     template <typename T>
