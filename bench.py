@@ -30,6 +30,7 @@ METRIC = "Darcy solve s @1e-10 vs FP64 oracle: FP32-refined vs FP64 GPU; HBM GB/
 CACHE = os.path.join(ROOT, "wsl-code_b200", "_meshcache")
 INNER_TOL = 1e-6  # FP32 inner MINRES: relative reduction per refinement step
 PARITY_TOL = 1e-12  # residual of the solves compared with the oracle
+FD_TOL = 1e-14  # residual of the FP64 solves of the finite-difference and gradient checks (the FP64 floor)
 
 
 def parse():
@@ -42,6 +43,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--cpu-sample-cells", type=int, default=8000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-oracle-checks", action="store_true", help="skip the oracle's LU checks of C2 and C4")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--profile", action="store_true", help="short fixed run for profilers (applies + 2 solves)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient workload")
@@ -53,6 +55,7 @@ def parse():
     ap.add_argument("--no-ms", action="store_true", help="skip the Maxwell-Stefan leg")
     ap.add_argument("--ms-steps", type=int, default=100)
     ap.add_argument("--eager", action="store_true", help="with --profile: host-driven Krylov batches, no graph")
+    ap.add_argument("--profile-ms", action="store_true", help="with --profile: also Maxwell-Stefan applies and steps")
     return ap.parse_args()
 
 
@@ -330,17 +333,20 @@ class OracleJob:
                 self.p.terminate()
 
 
-def adjoint_leg(args, rank):
-    """Gradient workload (250k-cell annulus, lognormal K): J = sum over 64 seeded interior points of
-    (p_h - d)^2, the data d being the pressures of a solve with a second seeded K field. Reports the
-    adjoint (vg_adjoint_grad: adjoint solve + per-cell contraction) against the forward solve, both
-    device-timed, and FP64 central differences (step 1e-6, solves to 1e-12) of J along 20 seeded unit
-    directions against the adjoint's directional derivatives."""
+def adjoint_leg(args, rank, job=None):
+    """Config C4 (250k-cell annulus, lognormal K): J = sum over 64 seeded interior points of
+    (p_h - d)^2, the data d being the pressures of a solve with a second seeded K field. Reports:
+    * the adjoint (vg_adjoint_grad: adjoint solve + per-cell contraction) against the forward
+      solve, both device-timed, in mixed and FP64 modes (solves to 1e-10);
+    * the gradient from solves to FD_TOL against the oracle's CPU FP64 gradient (sparse LU of the
+      forward system, adjoint by the transposed factors, per-cell contraction; `job`);
+    * FP64 central differences (step 1e-6) of J along 20 seeded unit directions, each J from a
+      solve to FD_TOL started from the base solution, against the adjoint's directional derivatives,
+      relative to the largest directional derivative."""
     import numpy as np
     import torch
     import vemgpu
     from vemgpu import fields, observe
-    from vemgpu.autograd import darcy_solve
     cells = args.adjoint_cells
     mesh, _ = annulus_problem(cells, args.seed)
     cen = fields.cell_centroids(mesh)
@@ -350,6 +356,8 @@ def adjoint_leg(args, rank):
     obs = observe.PointObservation(h, mesh, observe.seeded_points(64, args.seed + 12))
     xd, _ = h.solve(tol=1e-12)
     obs.data = obs.pressure(xd).clone()
+    if job is not None:
+        job.send((obs.index.cpu().numpy(), obs.data.cpu().numpy()))
     h.set_log_permeability(th)
     out = {"cells": h.nc, "observations": 64, "data": "pressures of a second seeded K field"}
     for mode in ("mixed", "fp64"):
@@ -366,28 +374,47 @@ def adjoint_leg(args, rank):
         out[mode] = {"forward_s": float(np.mean(fw)), "adjoint_s": float(np.mean(ad)),
                      "grad_over_solve": float(np.mean(ad) / np.mean(fw)),
                      "forward_iterations": info["iterations"], "adjoint_iterations": ainfo["iterations"]}
-    theta = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
-    J = obs(darcy_solve(h, theta, tol=1e-12))
-    J.backward()
-    gn = float(torch.linalg.norm(theta.grad))
+
+    def solve_tight(guess=None):
+        x = h.zeros() if guess is None else guess.clone()
+        try:
+            _, info = h.solve(x=x, mode="fp64", tol=FD_TOL, guess=guess is not None)
+            return x, info["residual"]
+        except vemgpu.VemGpuError:
+            return x, float("nan")  # the FP64 floor was reached before FD_TOL: x is the last iterate
+    x0, res0 = solve_tight()
+    J = float(obs(x0))
+    dJdx = torch.autograd.functional.vjp(obs, x0)[1]
+    grad, ginfo = h.adjoint_grad(x0, dJdx, mode="fp64", tol=FD_TOL)
+    gn = float(torch.linalg.norm(grad))
+    out["J"], out["grad_norm"], out["tight_residual"] = J, gn, res0
+    if job is not None:
+        r = job.recv()
+        gc = r["g"]
+        gg = grad.cpu().numpy()
+        out["cpu_gradient"] = {"max_abs_diff_over_max_abs": float(np.abs(gg - gc).max() / np.abs(gc).max()),
+                               "J_rel_diff": abs(J - r["J"]) / abs(r["J"]), "oracle_seconds": r["seconds"],
+                               "oracle": "sparse LU of the 1M-unknown system, adjoint by the transposed factors"}
+        job.close()
     rng = np.random.default_rng(args.seed + 14)
     ad, fd = [], []
     t0 = time.time()
-    with torch.no_grad():
-        for _ in range(args.fd_directions):
-            v = torch.tensor(rng.standard_normal(h.nc), device="cuda")
-            v = v / torch.linalg.norm(v)
-            jp = float(obs(darcy_solve(h, theta + 1e-6 * v, tol=1e-12)))
-            jm = float(obs(darcy_solve(h, theta - 1e-6 * v, tol=1e-12)))
-            ad.append(float(theta.grad @ v))
-            fd.append((jp - jm) / 2e-6)
+    base = torch.tensor(th, dtype=torch.float64, device="cuda")
+    for _ in range(args.fd_directions):
+        v = torch.tensor(rng.standard_normal(h.nc), device="cuda")
+        v = v / torch.linalg.norm(v)
+        h.set_log_permeability(base + 1e-6 * v)
+        jp = float(obs(solve_tight(x0)[0]))
+        h.set_log_permeability(base - 1e-6 * v)
+        jm = float(obs(solve_tight(x0)[0]))
+        ad.append(float(grad @ v))
+        fd.append((jp - jm) / 2e-6)
+    h.set_log_permeability(base)
     ad, fd = np.array(ad), np.array(fd)
-    out["fd_check"] = {"directions": len(ad), "step": 1e-6,
+    out["fd_check"] = {"directions": len(ad), "step": 1e-6, "solve_tol": FD_TOL,
                        "max_abs_diff_over_max_abs_derivative": float(np.abs(ad - fd).max() / np.abs(ad).max()),
                        "max_abs_diff_over_grad_norm": float(np.abs(ad - fd).max() / gn),
                        "seconds": time.time() - t0}
-    out["grad_norm"] = gn
-    out["J"] = float(J.detach())
     h.close()
     return out
 
@@ -412,24 +439,28 @@ def assembled_leg(g, z32, z64, stream_ms):
 
 def ms_leg(args):
     """Ternary Maxwell-Stefan on the 250k-cell disk: D12 = 1, D13 = 0.5, D23 = 0.2, seeded smooth
-    initial fractions in [0.1, 0.8] summing to 1, backward Euler dt = 1e-3, 100 steps; FP64 and
-    FP32-refined runs (each step to 1e-10), sum-to-one, bounds and species masses checked every step."""
+    initial fractions in [0.1, 0.8] summing to 1, backward Euler dt = 1e-3, 100 steps, each step
+    fully implicit: Picard iterations on the friction matrix to relative change 1e-9 (the
+    reference's default --picard-tol), every linear system to 1e-10; FP64 and FP32-refined runs,
+    sum-to-one, bounds and species masses checked every step."""
     import numpy as np
     import torch
     from vemgpu.maxwell_stefan import MaxwellStefan, initial_fractions
     mesh = disk_mesh(args.config1_cells, args.seed)
-    ms = MaxwellStefan(mesh, D=(1.0, 0.5, 0.2), dt=1e-3)
+    ms = MaxwellStefan(mesh, D=(1.0, 0.5, 0.2), dt=1e-3, picard=50, picard_tol=1e-9)
     x1, x2, _ = initial_fractions(mesh, seed=args.seed + 31)
     s0 = ms.state(x1, x2)
     m0 = ms.masses(s0)
-    out = {"cells": ms.nc, "unknowns": ms.N, "steps": args.ms_steps, "dt": 1e-3, "D": [1.0, 0.5, 0.2]}
+    out = {"cells": ms.nc, "unknowns": ms.N, "steps": args.ms_steps, "dt": 1e-3, "D": [1.0, 0.5, 0.2],
+           "step": "backward Euler, fully implicit by Picard iterations on the friction matrix (tol 1e-9)"}
     finals = {}
     for mode in ("fp64", "mixed"):
         s = s0.clone()
-        its, secs, sum_err, mass_err, lo, hi = [], [], 0.0, 0.0, 1.0, 0.0
+        its, secs, pics, sum_err, mass_err, lo, hi = [], [], [], 0.0, 0.0, 1.0, 0.0
         for _ in range(args.ms_steps):
             s, info = ms.step(s, mode=mode, tol=1e-10, inner_tol=1e-5)
             its.append(info["iterations"])
+            pics.append(info["picard"])
             secs.append(info["seconds"])
             f = ms.fractions(s)
             sum_err = max(sum_err, float(torch.abs(f[0] + f[1] + f[2] - 1).max()))
@@ -439,6 +470,7 @@ def ms_leg(args):
         finals[mode] = torch.cat(ms.fractions(s)[:2])
         out[mode] = {"total_s": float(np.sum(secs)), "step_ms_mean": 1e3 * float(np.mean(secs)),
                      "iterations_mean": float(np.mean(its)), "iterations_max": int(np.max(its)),
+                     "picard_mean": float(np.mean(pics)), "picard_max": int(np.max(pics)),
                      "max_sum_to_one_error": sum_err, "max_rel_mass_change": mass_err, "min_fraction": lo,
                      "max_fraction": hi}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["total_s"] / out["mixed"]["total_s"]
@@ -560,8 +592,9 @@ def c2_leg(args, job):
         if k == 1 and job is not None:
             job.send(xp.cpu().numpy())
             r = job.recv()
+            ep = g.errors(xp)
             row["oracle_residual_of_gpu_solution"] = r["residual"]
-            row["oracle_vs_gpu_l2_pressure"] = abs(r["errors"]["scalar_phys"] / e["scalar_phys"] - 1)
+            row["oracle_vs_gpu_l2_pressure_rel"] = abs(r["errors"]["scalar_phys"] / ep["scalar_phys"] - 1)
         out[f"k{k}"] = row
         g.close()
     if job is not None:
@@ -602,6 +635,17 @@ def ours(args, rank, world, dist):
     mesh, _ = annulus_problem(args.cells, args.seed)
     from vemgpu import fields
     theta = fields.gaussian_field(fields.cell_centroids(mesh), sigma=2.0, corr=0.1, seed=replica_seed(args.seed, rank))
+    # the oracle's CPU checks of configs C2 and C4 (sparse LU of 1M-unknown systems, minutes of one
+    # core each) run in spawned processes beside the GPU legs; rank 0 of a single-GPU run only
+    jobs = {}
+    if rank == 0 and world == 1 and not args.profile and not args.no_oracle_checks:
+        if not args.no_config1:
+            disk_mesh(args.config1_cells, args.seed)
+            jobs["c2"] = OracleJob("c2", os.path.join(CACHE, f"disk_{args.config1_cells}_s{args.seed}.npz"))
+        if not args.no_adjoint:
+            amesh, _ = annulus_problem(args.adjoint_cells, args.seed)
+            ath = fields.gaussian_field(fields.cell_centroids(amesh), sigma=2.0, corr=0.1, seed=args.seed + 11)
+            jobs["c4"] = OracleJob("c4", os.path.join(CACHE, f"annulus_{args.adjoint_cells}_s{args.seed}.npz"), ath)
     t0 = time.time()
     g = vemgpu.DarcyGpu(mesh, k=0, nq=9, ng=9, geometry="arcs", problem="annulus", bc="pressure", theta=theta)
     setup_s = time.time() - t0
@@ -620,6 +664,22 @@ def ours(args, rank, world, dist):
         g.solve(b, x, mode="fp64", tol=1e-10, check_every=ce)
         g.solve(b, x, mode="mixed", tol=1e-10, inner_tol=INNER_TOL, check_every=ce)
         torch.cuda.synchronize()
+        if args.profile_ms:
+            # Maxwell-Stefan kernels: 3 FP64 and 3 FP32 applies, one FP64 and one mixed step, on a
+            # disk of the same cell count
+            from vemgpu.maxwell_stefan import MaxwellStefan, initial_fractions
+            dm = disk_mesh(args.cells, args.seed)
+            ms = MaxwellStefan(dm, D=(1.0, 0.5, 0.2), dt=1e-3)
+            x1, x2, _ = initial_fractions(dm, seed=args.seed + 31)
+            st = ms.state(x1, x2)
+            zz = torch.randn(ms.N, dtype=torch.float64, device="cuda")
+            for _ in range(3):
+                ms.apply(st, zz)
+                ms.apply(st, zz.float())
+            for mode in ("fp64", "mixed"):
+                ms.step(st, mode=mode, tol=1e-10, inner_tol=1e-5)
+            torch.cuda.synchronize()
+            ms.close()
         print(json.dumps({"profile": "done", "cells": g.nc, "dofs": g.N}), flush=True)
         return
 
@@ -658,6 +718,20 @@ def ours(args, rank, world, dist):
                            speedup_mixed_vs_fp64=ms64 / ms_mixed)
         x64 = x.clone()
         res["fp64"]["rel_diff_mixed_vs_fp64"] = float(torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64))
+        # FP64 reference of the 1M-cell workload (the oracle's sparse LU does not reach this size):
+        # the FP64 solve driven to the FP64 floor, true residual 1e-14
+        xr = g.zeros()
+        try:
+            _, ir = g.solve(b, xr, mode="fp64", tol=1e-14)
+            ref_res = ir["residual"]
+        except vemgpu.VemGpuError:
+            ref_res = float("nan")
+        nr = torch.linalg.norm(xr)
+        res["accuracy"] = {"reference": "FP64 GPU solve to true relative residual 1e-14",
+                           "reference_residual": ref_res,
+                           "mixed_rel_err": float(torch.linalg.norm(x_mixed - xr) / nr),
+                           "fp64_rel_err": float(torch.linalg.norm(x64 - xr) / nr), "target": 1e-10}
+        del xr
     # per-kernel device times on the same buffers (FP32 apply, FP64 apply) with L2 flushed in between
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     z32 = torch.randn(g.N, dtype=torch.float32, device="cuda")
@@ -722,8 +796,8 @@ def ours(args, rank, world, dist):
         if i:
             e2e.append(time.perf_counter() - t)
     e2e_s = max_over_ranks(sum(e2e) / len(e2e), dist)
-    adjoint = None if args.no_adjoint else adjoint_leg(args, rank)
-    config1 = None if args.no_config1 else c2_leg(args, None)
+    adjoint = None if args.no_adjoint else adjoint_leg(args, rank, jobs.get("c4"))
+    config1 = None if args.no_config1 else c2_leg(args, jobs.get("c2"))
     c1 = None if args.no_config1 else c1_leg(args)
     ms = None if args.no_ms else ms_leg(args)
     cpu = same = None
@@ -769,12 +843,53 @@ def ours(args, rank, world, dist):
         "disk_250k": config1,
         "disk_1k": c1,
         "maxwell_stefan": ms,
+        "same_size": same,
         "gpu_launches": launches,
         "clocks": clocks,
-        "same_size": same,
         "cpu_baseline": cpu,
     }
+    line["summary"] = summary(line)  # last: the figures a reader of the line's end needs
     print(json.dumps(line), flush=True)
+
+
+def summary(line):
+    """The headline figures of every leg in a few keys (the end of the JSON line)."""
+    def get(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict) or d.get(k) is None:
+                return None
+            d = d[k]
+        return d
+
+    def r(v, n=3):
+        return None if v is None else float(f"{v:.{n}g}")
+    f = line.get("fp64") or {}
+    out = {"mixed_s": r(line["value"]), "fp64_s": r(f.get("solve_s")),
+           "mixed_over_fp64": r(f.get("speedup_mixed_vs_fp64")),
+           "mixed_err_vs_fp64_ref": r(get(f, "accuracy", "mixed_rel_err")),
+           "apply_fp32_frac": r(line["roofline"]["frac"]), "apply_fp64_frac": r(line["roofline"]["fp64_apply_frac"]),
+           "e2e_s": r(line["e2e"]["value"])}
+    a = line.get("adjoint")
+    if a:
+        out.update(grad_over_solve=r(get(a, "mixed", "grad_over_solve")),
+                   grad_vs_cpu=r(get(a, "cpu_gradient", "max_abs_diff_over_max_abs")),
+                   fd_vs_max_derivative=r(get(a, "fd_check", "max_abs_diff_over_max_abs_derivative")))
+    c2 = line.get("disk_250k")
+    if c2:
+        out.update(c2_k0_err_vs_lu=r(get(c2, "k0", "mixed", "rel_err_vs_oracle_lu_at_1e-10")),
+                   c2_k1_oracle_residual=r(get(c2, "k1", "oracle_residual_of_gpu_solution")))
+    c1 = line.get("disk_1k")
+    if c1:
+        out.update(c1_err_vs_lu=r(get(c1, "mixed", "rel_err_vs_lu")), c1_cpu_s=r(get(c1, "cpu_reference", "seconds")),
+                   c1_l2_p=r(get(c1, "cpu_reference", "l2_pressure")), c1_l2_u=r(get(c1, "cpu_reference", "l2_flux")))
+    ss = line.get("same_size")
+    if ss:
+        out.update(same_size_cells=ss["cells"], same_size_cpu_over_gpu_solve=r(ss["ratio_solve_vs_mixed"]),
+                   same_size_cpu_over_gpu_e2e=r(ss["ratio_e2e"]))
+    ms = line.get("maxwell_stefan")
+    if ms:
+        out.update(ms_mixed_s=r(get(ms, "mixed", "total_s")), ms_fp64_s=r(get(ms, "fp64", "total_s")))
+    return out
 
 
 def main():

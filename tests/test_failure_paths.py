@@ -130,9 +130,11 @@ def test_nonpositive_jacobian_reported():
 @pytest.mark.gpu
 def test_singular_local_matrix_reported():
     torch, vemgpu = _gpu()
-    # a sliver quadrilateral of relative area 1e-30: its local Gram matrices have pivots far below
-    # the inverse's singular threshold
-    xy = np.array([[0, 0], [1, 0], [1, 1e-30], [0, 1e-30]], float)
+    # a square of side 1e-15 (area 1e-30): the pivots of its scaled-monomial mass matrix H are of
+    # the size of the area, far below the inverse's absolute singular threshold 1e-28 (the
+    # reference's, vem/CurvedVEM_Darcy_gpu/include/device.cuh:243-244)
+    s = 1e-15
+    xy = np.array([[0, 0], [s, 0], [s, s], [0, s]], float)
     mesh = dict(xy=xy, cell_ptr=np.array([0, 4], np.int32), cell_nodes=np.array([0, 1, 2, 3], np.int32))
     with pytest.raises(L.VemGpuError) as e:
         vemgpu.DarcyGpu(mesh, k=1, geometry="identity", problem="sincos", bc="flux")

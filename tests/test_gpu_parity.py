@@ -4,8 +4,9 @@ reference's golden results. Tolerances are written in each test:
 * FP64 local operators and apply: relative 1e-12 (same FP64 mathematics, different summation
   order and the reference GPU's exact edge moments instead of edge quadrature);
 * FP32 operator: relative 2e-6 of the FP64 result;
-* solutions: relative 2-norm difference to the oracle's sparse-LU solution, given per test from
-  the solve tolerance;
+* solutions: relative 2-norm difference to the oracle's sparse-LU solution at most 1e-10 (the
+  discrete-solution target), for solves to the reference's true-residual tolerance 1e-10 on the
+  C1 disk and the lognormal annuli, and to 1e-12 where the test says so;
 * golden error figures: the oracle's own tolerances (tests/test_oracle_golden.py).
 """
 import numpy as np
@@ -181,24 +182,28 @@ def test_golden_reports_on_gpu(golden, square_meshes):
 def test_solution_matches_oracle_flux_bc(square_meshes, name, k):
     o, g = pair(square_meshes[name], k, 9, O.GEOM_SINE, 0.05, O.PROB_SINCOS, O.BC_FLUX)
     xo, _, _ = o.solve_direct()
-    x, info = g.solve(tol=1e-12)
+    x, info = g.solve(tol=1e-12)  # essential flux BC with the multiplier: solved to 1e-12
     assert info["residual"] <= 1e-12
     xg = x.cpu().numpy()
-    assert np.linalg.norm(xg - xo) <= 1e-9 * np.linalg.norm(xo)
+    assert np.linalg.norm(xg - xo) <= 1e-10 * np.linalg.norm(xo)
     eo, eg = o.errors(xo), g.errors(x)
     for key in eo:
         assert eg[key] == pytest.approx(eo[key], rel=1e-8, abs=1e-12), key
 
 
 @pytest.mark.parametrize("k", [0, 1])
-def test_solution_matches_oracle_disk(k):
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_solution_matches_oracle_disk(k, mode):
+    """Config C1's disk (1000 Voronoi cells, exact arcs, p = sin(pi x) sin(pi y), Dirichlet
+    pressure): a solve to the reference's true-residual tolerance 1e-10 is within 1e-10 of the
+    oracle's sparse-LU solution, FP64 and FP32-refined."""
     m = meshgen.voronoi_mesh(1000, "disk", seed=2)
     o, g = pair(m, k, 9, O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
     xo, _, _ = o.solve_direct()
-    x, info = g.solve(tol=1e-10)
+    x, info = g.solve(tol=1e-10, mode=mode)
     assert info["residual"] <= 1e-10
     xg = x.cpu().numpy()
-    assert np.linalg.norm(xg - xo) <= 1e-8 * np.linalg.norm(xo)
+    assert np.linalg.norm(xg - xo) <= 1e-10 * np.linalg.norm(xo)
     # the error kernel reproduces the oracle's figures on the same vector
     eo, eg = o.errors(xg), g.errors(x)
     for key in eo:
@@ -213,7 +218,7 @@ def test_mixed_precision_refinement(annulus300):
     assert i64["residual"] <= 1e-10 and im["residual"] <= 1e-10
     xo, _, _ = o.solve_direct()
     for x in (x64, xm):
-        assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+        assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-10 * np.linalg.norm(xo)
 
 
 def test_solve_host_matches_device(annulus300):
@@ -225,18 +230,26 @@ def test_solve_host_matches_device(annulus300):
     assert np.array_equal(xd.cpu().numpy(), xh)
 
 
-def test_multigrid_solve_matches_oracle_30k():
-    """k = 0 with the pressure condition at 30,000 cells: a multigrid hierarchy of several levels
-    (30k -> ~3.3k -> dense coarsest) preconditions the pressure block."""
+@pytest.mark.parametrize("field", ["lognormal", "iid"])
+def test_multigrid_solve_matches_oracle_30k(field):
+    """k = 0 with the pressure condition at 30,000 cells of the workload's annulus: a multigrid
+    hierarchy of several levels (30k -> ~3.3k -> dense coarsest) preconditions the pressure block.
+    The lognormal field is the workload's (Gaussian random field, exponential covariance, sigma 2,
+    correlation length 0.1); solves to the true-residual tolerance 1e-10 are within 1e-10 of the
+    oracle's sparse-LU solution, FP64 and FP32-refined."""
+    from vemgpu import fields
     m = meshgen.voronoi_mesh(30000, "annulus", seed=61)
-    th = np.random.default_rng(62).normal(0, 1.5, 30000)
+    if field == "lognormal":
+        th = fields.gaussian_field(fields.cell_centroids(m), sigma=2.0, corr=0.1, seed=5)
+    else:
+        th = np.random.default_rng(62).normal(0, 1.5, 30000)
     o, g = pair(m, 0, 9, O.GEOM_ARCS, 0.0, O.PROB_ANNULUS, O.BC_PRESSURE, theta=th)
     xo, _, _ = o.solve_direct()
     for mode in ("fp64", "mixed"):
         x, info = g.solve(tol=1e-10, mode=mode)
         assert info["residual"] <= 1e-10
         assert info["iterations"] < 200, info
-        assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+        assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-10 * np.linalg.norm(xo)
 
 
 def test_multigrid_k1_solve_matches_oracle_20k():
@@ -247,10 +260,10 @@ def test_multigrid_k1_solve_matches_oracle_20k():
     o, g = pair(m, 1, 9, O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
     xo, _, _ = o.solve_direct()
     for mode in ("fp64", "mixed"):
-        x, info = g.solve(tol=1e-10, mode=mode)
-        assert info["residual"] <= 1e-10
-        assert info["iterations"] < 400, info
-        assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+        x, info = g.solve(tol=1e-12, mode=mode)  # solved to 1e-12
+        assert info["residual"] <= 1e-12
+        assert info["iterations"] < 700, info
+        assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-10 * np.linalg.norm(xo)
 
 
 def test_vtk_file_handle_matches_dict_handle(tmp_path, disk200):
@@ -317,9 +330,9 @@ def test_multigrid_high_order_pressure_bc(k):
     m = meshgen.voronoi_mesh(1500, "disk", seed=64 + k)
     o, g = pair(m, k, default_nq(k), O.GEOM_ARCS, 0.0, O.PROB_SINSIN, O.BC_PRESSURE)
     xo, _, _ = o.solve_direct()
-    x, info = g.solve(tol=1e-10)
-    assert info["residual"] <= 1e-10
-    assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+    x, info = g.solve(tol=1e-12)  # solved to 1e-12
+    assert info["residual"] <= 1e-12
+    assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-10 * np.linalg.norm(xo)
 
 
 def test_calls_run_on_the_handles_device():
@@ -346,3 +359,26 @@ def test_calls_run_on_the_handles_device():
         assert torch.cuda.current_device() == other
     finally:
         torch.cuda.set_device(0)
+
+
+@pytest.mark.parametrize("k,order", [(0, 1.0), (1, 2.0)])
+def test_disk_convergence_orders(k, order):
+    """Manufactured solution p = sin(pi x) sin(pi y) on the curved disk (exact arcs, Dirichlet
+    pressure), four Voronoi meshes with h halving: the physical pressure and flux L2 errors fall as
+    h^(k+1) (the reference pins its square meshes the same way,
+    vem/CurvedVEM_Darcy/results_darcy_convergence_k1.txt:7-13). Slopes within 0.25 of k + 1."""
+    hs, ep, eu = [], [], []
+    for n in (500, 2000, 8000, 32000):
+        m = meshgen.voronoi_mesh(n, "disk", seed=81)
+        g = vemgpu.DarcyGpu(m, k=k, geometry="arcs", problem="sinsin", bc="pressure")
+        x, info = g.solve(tol=1e-12)
+        assert info["residual"] <= 1e-12
+        e = g.errors(x)
+        hs.append(np.sqrt(np.pi / n))
+        ep.append(e["scalar_phys"])
+        eu.append(e["flux_phys"])
+        g.close()
+    lh = np.log(hs)
+    for err in (ep, eu):
+        slope = np.polyfit(lh, np.log(err), 1)[0]
+        assert abs(slope - order) <= 0.25, (slope, err)

@@ -198,8 +198,12 @@ __device__ __forceinline__ void cell_apply(const ApplyArgs<T>& a, const Src& src
         }
     }
     if (a.red) {
+        // the cell's share of delta = x^T K x, summed in the operator's precision and promoted
+        // once (an FP32 inner solve needs no FP64 products; fewer conversions per cell)
+        T qc = T(0);
 #pragma unroll
-        for (int i = 0; i < N; ++i) quad += double(u[i]) * double(yu[i]);
+        for (int i = 0; i < N; ++i) qc += u[i] * yu[i];
+        quad += double(qc);
     }
     T yp[Q];
 #pragma unroll
@@ -220,9 +224,11 @@ __device__ __forceinline__ void cell_apply(const ApplyArgs<T>& a, const Src& src
                 yp[r] += w * u[i];
             }
     }
-    if (a.red) {
+    if (a.red && a.psign != T(1)) {
+        T qp = T(0);
 #pragma unroll
-        for (int r = 0; r < Q; ++r) quad += (double(a.psign) - 1.0) * double(pr[r]) * double(yp[r]);
+        for (int r = 0; r < Q; ++r) qp += pr[r] * yp[r];
+        quad += (double(a.psign) - 1.0) * double(qp);
     }
 #pragma unroll
     for (int i = 0; i < ED; ++i) {
