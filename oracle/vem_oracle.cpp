@@ -1353,7 +1353,10 @@ int orc_reference_solve(int nn, const double* xy, int nc, const int* cell_ptr, c
         int N = o->N;
         std::vector<int> mask(N, 0);
         std::vector<double> g(N, 0.0);
-        orc_boundary(o, mask.data(), g.data());
+        // essential flux rows only for the flux condition (DarcySolver::solveWithDirichletBC,
+        // C/solver/DarcySolver.cpp:665-788); the pressure condition enters as a load on the flux
+        // rows and keeps every row
+        if (o->bc == BC_FLUX) orc_boundary(o, mask.data(), g.data());
         std::vector<double> kg(N);
         spmv(full, g.data(), kg.data());
         std::vector<int> fidx, inv(N, -1);

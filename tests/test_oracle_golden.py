@@ -123,3 +123,21 @@ def test_projector_identities(square_meshes, k):
         A = o.local(c, "A").reshape(n, n)
         np.testing.assert_allclose(A, A.T, atol=1e-12 * np.abs(A).max())
         assert np.linalg.eigvalsh(A).min() > 0
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_reference_cpu_solver_matches_direct_solve(k):
+    """The timed CPU baseline (the reference's GMRES(100) + ILU(0), rtol 1e-10, restated in the
+    oracle after vem/CurvedVEM_Darcy/core/petsc_utils.cpp:144-211) solves the same system as the
+    oracle's sparse LU. Like PETSc's default GMRES it stops on the left-preconditioned residual
+    (1e-10), which leaves a true residual up to ~1e-9 and solution errors of 1e-10 to 1e-8 on this
+    disk: bounds 1e-8 and 1e-7."""
+    import meshgen_ref
+    m = meshgen_ref.voronoi_mesh(1000, "disk", seed=2)
+    o = O.Oracle(m, k=k, nq=9, ng=9, geom=O.GEOM_ARCS, problem=O.PROB_SINSIN, bc=O.BC_PRESSURE)
+    xo, K, b = o.solve_direct()
+    x, it, tm = O.reference_solve(m, k=k, nq=9, ng=9, geom=O.GEOM_ARCS, problem=O.PROB_SINSIN, bc=O.BC_PRESSURE,
+                                  threads=1, rtol=1e-10)
+    assert it > 0 and tm["rel"] <= 1e-10
+    assert np.linalg.norm(b - K @ x) <= 1e-8 * np.linalg.norm(b)
+    assert np.linalg.norm(x - xo) <= 1e-7 * np.linalg.norm(xo)
