@@ -413,10 +413,16 @@ def adjoint_leg(args, rank, job=None):
         fd.append((jp - jm) / 2e-6)
     h.set_log_permeability(base)
     ad, fd = np.array(ad), np.array(fd)
+    # rounding floor of a central difference of J: one unit in the last place of J in each of the
+    # two values, divided by 2 step; relative to the largest directional derivative
+    ulp = float(np.spacing(abs(J)))
+    floor = ulp / 2e-6 / np.abs(ad).max()
+    err = float(np.abs(ad - fd).max() / np.abs(ad).max())
     out["fd_check"] = {"directions": len(ad), "step": 1e-6, "solve_tol": FD_TOL,
-                       "max_abs_diff_over_max_abs_derivative": float(np.abs(ad - fd).max() / np.abs(ad).max()),
+                       "max_abs_diff_over_max_abs_derivative": err,
                        "max_abs_diff_over_grad_norm": float(np.abs(ad - fd).max() / gn),
-                       "seconds": time.time() - t0}
+                       "rounding_floor_over_max_abs_derivative": floor, "error_in_floor_units": err / floor,
+                       "max_abs_derivative": float(np.abs(ad).max()), "seconds": time.time() - t0}
     h.close()
     return out
 
@@ -829,6 +835,7 @@ def ours(args, rank, world, dist):
         "throughput": {"solves_per_s": world / (ms_mixed * 1e-3), "replicas": world},
         "iterations": info_mixed[0]["iterations"], "outer": info_mixed[0]["outer"],
         "residual": info_mixed[0]["residual"], "setup_s": setup_s, "fp64": res.get("fp64"),
+        "accuracy": res.get("accuracy"),
         "kernels": {"apply_fp32_ms": apply32_ms, "apply_fp64_ms": apply64_ms, "apply_fp32_bytes": b32,
                     "apply_fp64_bytes": b64, "apply_fp32_flushed_ms": apply32_flushed_ms,
                     "apply_fp64_flushed_ms": apply64_flushed_ms,
@@ -868,14 +875,15 @@ def summary(line):
     f = line.get("fp64") or {}
     out = {"mixed_s": r(line["value"]), "fp64_s": r(f.get("solve_s")),
            "mixed_over_fp64": r(f.get("speedup_mixed_vs_fp64")),
-           "mixed_err_vs_fp64_ref": r(get(f, "accuracy", "mixed_rel_err")),
+           "mixed_err_vs_fp64_ref": r(get(line, "accuracy", "mixed_rel_err")),
            "apply_fp32_frac": r(line["roofline"]["frac"]), "apply_fp64_frac": r(line["roofline"]["fp64_apply_frac"]),
            "e2e_s": r(line["e2e"]["value"])}
     a = line.get("adjoint")
     if a:
         out.update(grad_over_solve=r(get(a, "mixed", "grad_over_solve")),
                    grad_vs_cpu=r(get(a, "cpu_gradient", "max_abs_diff_over_max_abs")),
-                   fd_vs_max_derivative=r(get(a, "fd_check", "max_abs_diff_over_max_abs_derivative")))
+                   fd_vs_max_derivative=r(get(a, "fd_check", "max_abs_diff_over_max_abs_derivative")),
+                   fd_floor=r(get(a, "fd_check", "rounding_floor_over_max_abs_derivative")))
     c2 = line.get("disk_250k")
     if c2:
         out.update(c2_k0_err_vs_lu=r(get(c2, "k0", "mixed", "rel_err_vs_oracle_lu_at_1e-10")),
