@@ -527,39 +527,58 @@ void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, 
     }
 }
 
-// coarsest level: z = Ainv b, one block of TPB threads per row (enough warps in flight per SM
-// for a matrix of up to COARSE_MAX^2 entries), fixed-order block reduction
+// coarsest level: z = Ainv b, one warp per row. The inverse does not change between cycles: its
+// rows are loaded with an L2 evict-last hint, so that they stay resident in L2 while the operator
+// records stream through with evict-first, and each warp loads its row into registers before the
+// programmatic-launch wait (while the restriction before it still runs). After the wait only b is
+// read. Lane l sums the entries l, l + 32, ... in order, then a fixed shuffle tree: deterministic.
+constexpr int DENSE_WARPS = 4;  // rows per block
 template <typename T>
-__global__ void __launch_bounds__(TPB) k_dense(int n, const T* Ainv, const T* b, T* z) {
-    __shared__ T sh[TPB / 32];
+struct DensePre {
+    static constexpr int value = sizeof(T) == 4 ? 72 : 36;  // entries per lane held in registers
+};
+
+template <typename T>
+__device__ __forceinline__ T ld_keep(const T* p, unsigned long long pol);
+template <>
+__device__ __forceinline__ float ld_keep<float>(const float* p, unsigned long long pol) {
+    float v;
+    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+template <>
+__device__ __forceinline__ double ld_keep<double>(const double* p, unsigned long long pol) {
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(DENSE_WARPS * 32) k_dense(int n, const T* Ainv, const T* b, T* z) {
     pdl_trigger();
-    const int row = blockIdx.x, t = threadIdx.x;
-    const T* a = Ainv + (long long)row * n;
-    // the row of the inverse does not depend on earlier kernels: load it before the wait
-    constexpr int PRE = (DENSE_MAX + TPB - 1) / TPB;
+    constexpr int PRE = DensePre<T>::value;
+    const int lane = threadIdx.x & 31, row = blockIdx.x * DENSE_WARPS + (threadIdx.x >> 5);
+    const bool live = row < n;
+    const T* a = Ainv + (long long)(live ? row : 0) * n;
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
     T av[PRE];
 #pragma unroll
     for (int q = 0; q < PRE; ++q) {
-        const int j = t + q * TPB;
-        av[q] = j < n ? __ldcs(a + j) : T(0);
+        const int j = lane + 32 * q;
+        av[q] = (live && j < n) ? ld_keep(a + j, pol) : T(0);
     }
     pdl_wait();
-    T acc0 = T(0), acc1 = T(0);
+    if (!live) return;
+    T acc = T(0);
 #pragma unroll
-    for (int q = 0; q < PRE; q += 2) {
-        const int j = t + q * TPB;
-        if (j < n) acc0 += av[q] * b[j];
-        if (q + 1 < PRE && j + TPB < n) acc1 += av[q + 1] * b[j + TPB];
+    for (int q = 0; q < PRE; ++q) {
+        const int j = lane + 32 * q;
+        if (j < n) acc += av[q] * b[j];
     }
-    T acc = acc0 + acc1;
+    for (int j = lane + 32 * PRE; j < n; j += 32) acc += ld_keep(a + j, pol) * b[j];
     for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-    if ((t & 31) == 0) sh[t >> 5] = acc;
-    __syncthreads();
-    if (t == 0) {
-        T v = T(0);
-        for (int w = 0; w < TPB / 32; ++w) v += sh[w];
-        z[row] = v;
-    }
+    if (lane == 0) z[row] = acc;
 }
 
 // ---- dense inverse of the (symmetric positive definite) coarsest matrix on the device: in-place
@@ -1049,7 +1068,7 @@ void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     if (l == int(levels_.size()) - 1) {
         const T* inv = sizeof(T) == 8 ? reinterpret_cast<const T*>(dinvc64_.data())
                                       : reinterpret_cast<const T*>(dinvc32_.data());
-        launch_pdl(k_dense<T>, ncoarse_, TPB, 0, s, ncoarse_, inv, b, z);
+        launch_pdl(k_dense<T>, (ncoarse_ + DENSE_WARPS - 1) / DENSE_WARPS, DENSE_WARPS * 32, 0, s, ncoarse_, inv, b, z);
         ++launches;
         return;
     }

@@ -977,7 +977,9 @@ void Solver::ms_step(const double* old_state, double* new_state, const vg_solve_
                 const double rn = rel * nb;
                 k_d2f<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(ms_.r.data(), ms_.r32.data(), Nm, 1.0 / rn);
                 double r_in = 0;
-                total += ms_gmres<float>(ms_.r32.data(), ms_.d32.data(), o.inner_tol, o.maxit - total, mres, &r_in);
+                // reduction asked of this FP32 solve: inner_tol, or less when less reaches tol
+                const double itol = std::min(0.5, std::max(o.inner_tol, 0.5 * o.tol / rel));
+                total += ms_gmres<float>(ms_.r32.data(), ms_.d32.data(), itol, o.maxit - total, mres, &r_in);
                 k_addf<<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(new_state, ms_.d32.data(), rn, Nm);
                 rel = true_residual(nullptr);
             }
