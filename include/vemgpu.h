@@ -161,11 +161,12 @@ int vg_build(vg_handle* h);
  * Replaces MixedGpu::apply (vem/CurvedVEM_Darcy_gpu/src/equation_gpu.cu:580-598). */
 int vg_apply(vg_handle* h, const void* x, void* y, int precision, int constrained, void* stream);
 
-/* Failure-path test hook (no counterpart in the reference): the next matrix-free apply of the
- * handle (k <= 1) leaves one operator batch uncopied, so that the waits of the CTA that owns it
- * run out after their one-second limit; the kernel then drains its copies, sets its error word and
- * returns, and the call that launched it reports VG_ECUDA as described for vg_apply and vg_solve.
- * The result of that apply is wrong. For tests of the error path only. */
+/* Failure-path test hook (no counterpart in the reference): in the next matrix-free apply of the
+ * handle (k <= 1) one consumer warp waits, at its CTA's last operator batch, on a barrier that
+ * nothing arrives on, so that its bounded wait runs out after the one-second limit; the kernel then
+ * drains its copies, sets its error word and returns, and the call that launched it reports
+ * VG_ECUDA as described for vg_apply and vg_solve. The result of that apply is wrong (the pieces
+ * of that batch are missing). For tests of the error path only. */
 int vg_debug_stall_apply(vg_handle* h);
 
 /* Internally the solver numbers the flux unknowns by first use in its cell layout and the pressure

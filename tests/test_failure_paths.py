@@ -1,7 +1,8 @@
 """Failure paths: every error the library detects comes back as a status code, and the handle
 stays usable afterwards. No test faults, traps or hangs the GPU: the device-side case makes one
-bounded wait of the streamed apply run out (a stage that nothing fills) through the test hook
-vg_debug_stall_apply, and checks that the kernel returns and the call reports VG_ECUDA.
+bounded wait of the streamed apply run out (a consumer waiting on a barrier that nothing arrives
+on) through the test hook vg_debug_stall_apply, and checks that the kernel returns and the call
+reports VG_ECUDA.
 
 Reference counterparts: the true-residual failure of Krylov::solve
 (vem/CurvedVEM_Darcy_gpu/src/krylov.cu:171-174), the singular-pivot status of the local inverse
@@ -143,9 +144,9 @@ def test_singular_local_matrix_reported():
 
 @pytest.mark.gpu
 def test_apply_wait_limit_reports_error_and_recovers():
-    """The streamed apply's copy pipeline: one stage never fills, the consumers' one-second waits
-    run out, the kernel drains and returns, vg_apply reports VG_ECUDA on the next call and
-    vg_solve at its end; afterwards the handle computes correct results again."""
+    """The streamed apply's pipeline: one consumer's one-second wait runs out, the kernel drains
+    its copies and returns, vg_apply reports VG_ECUDA on the next call and vg_solve at its end;
+    afterwards the handle computes correct results again."""
     torch, vemgpu = _gpu()
     from vemgpu import meshgen
     g = vemgpu.DarcyGpu(meshgen.voronoi_mesh(20000, "annulus", seed=74), k=0, geometry="arcs", problem="annulus",

@@ -394,7 +394,8 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
     // descriptor of the batch in each stage, written by the producer before its arrival on
     // full[s] (release) and read by the consumers after their wait (acquire)
     __shared__ int st_first[MAX_STAGES], st_count[MAX_STAGES], st_direct[MAX_STAGES];
-    __shared__ int abort_flag, issued_sh, stalled_sh;
+    __shared__ int abort_flag, issued_sh;
+    __shared__ __align__(8) unsigned long long never;  // test hook: a barrier nothing arrives on
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b0 = a.cta_batch[blockIdx.x], nb = a.cta_batch[blockIdx.x + 1] - b0;
     const int S = a.stages, SB = a.stage_bytes;
@@ -403,9 +404,9 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], BULK_CONSUMERS);
         }
+        mbar_init(&never, 1);
         abort_flag = 0;
         issued_sh = 0;
-        stalled_sh = -1;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -413,11 +414,6 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
     if (warp == 0) {
         if (lane == 0) {  // producer
             const unsigned long long pol = evict_first_policy();
-            // test hook (failure-path tests only): the first producer to find the flag set clears
-            // it and skips its last batch, whose stage then never fills; the flag is loaded here
-            // and first used at the last batch, so the load's latency stays off the stream
-            const int stall_req = a.stall ? *reinterpret_cast<volatile int*>(a.stall) : 0;
-            int stalled = -1;
             int issued = 0;
             bool ok = true;
             for (int i = 0; i < nb; ++i) {
@@ -430,16 +426,11 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
                 st_first[s] = B.first;
                 st_count[s] = B.count;
                 st_direct[s] = B.bytes == 0;
-                issued = i + 1;
-                if (i == nb - 1 && stall_req && atomicExch(a.stall, 0) != 0) {
-                    stalled = i;
-                    continue;
-                }
                 mbar_expect_tx(&full[s], unsigned(B.bytes));
                 if (B.bytes) bulk_g2s(ring + size_t(s) * SB, a.rec + B.off, unsigned(B.bytes), &full[s], pol);
+                issued = i + 1;
             }
             issued_sh = issued;
-            stalled_sh = stalled;
             if (!ok) {
                 abort_flag = 1;
                 atomicExch(a.err, 1);
@@ -447,9 +438,19 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
         }
     } else {  // consumers
         const int cw = warp - 1;
+        // test hook (failure-path tests only): the first consumer warp 0 to find the flag set
+        // clears it and, at its CTA's last batch, waits on a barrier nothing arrives on, so that
+        // its bounded wait runs out; the flag is loaded while the first stage is still in flight
+        int stall_req = 0;
+        if (cw == 0 && lane == 0 && a.stall) stall_req = *reinterpret_cast<volatile int*>(a.stall);
         for (int i = 0; i < nb; ++i) {
             const int s = i % S;
-            const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], unsigned(i / S) & 1u, &abort_flag));
+            bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], unsigned(i / S) & 1u, &abort_flag));
+            if (cw == 0 && i == nb - 1) {
+                int st = 0;
+                if (lane == 0 && stall_req) st = atomicExch(a.stall, 0);
+                if (__shfl_sync(0xffffffffu, st, 0)) ok = __all_sync(0xffffffffu, mbar_wait(&never, 0u, &abort_flag));
+            }
             if (!ok) {
                 if (lane == 0) {
                     abort_flag = 1;
@@ -477,8 +478,7 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
     if (abort_flag && threadIdx.x == 0) {
         // a wait gave up (producer or consumers): the copies still in flight (at most one per
         // stage, the last ones issued) land before the CTA exits; bounded as well
-        for (int i = max(0, issued_sh - S); i < issued_sh; ++i)
-            if (i != stalled_sh) mbar_wait(&full[i % S], unsigned(i / S) & 1u, nullptr);
+        for (int i = max(0, issued_sh - S); i < issued_sh; ++i) mbar_wait(&full[i % S], unsigned(i / S) & 1u, nullptr);
     }
     if (a.red || a.mult) finish_reduction<T, BULK_THREADS>(a, quad, msum);
 }

@@ -45,8 +45,8 @@ struct ApplyArgs {
     const int* cta_batch;  // batches of CTA c: [cta_batch[c], cta_batch[c + 1])
     int ncta, stages, stage_bytes;
     int* err;              // set to 1 when a pipeline wait gives up (never in a correct run)
-    int* stall;            // test hook: when nonzero, the first producer to see it clears it and
-                           // leaves its last batch uncopied, so that its consumers' waits run out
+    int* stall;            // test hook: when nonzero, the first consumer to see it clears it and
+                           // waits on a barrier nothing arrives on, so that its bounded wait runs out
 };
 
 constexpr int APPLY_THREADS = 256;

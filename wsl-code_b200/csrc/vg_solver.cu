@@ -955,8 +955,8 @@ void Solver::pack_streams(cudaStream_t s) {
     if (ref_streams_packed_) pack_streams_reference(s);  // new operator values (permeability update)
 }
 
-// Test hook of the failure path: the next streamed apply leaves one batch uncopied, so that the
-// consumers' bounded waits run out and the apply reports its error word.
+// Test hook of the failure path: in the next streamed apply one consumer's bounded wait runs out
+// (a barrier nothing arrives on) and the apply reports its error word.
 void Solver::inject_apply_stall() {
     if (k > 1 || !d_stall_.data()) throw Error(VG_ESTATE, "no streamed apply on this handle (k > 1)");
     const int one = 1;
