@@ -156,8 +156,9 @@ int vg_build(vg_handle* h);
  * precision VG_FP64 (double*) or VG_FP32 (float*). constrained = 1 applies the essential-BC mask
  * as Q A Q + (I - Q) (VG_BC_FLUX only). stream: cudaStream_t or NULL (legacy default stream).
  * Asynchronous: a failure inside the kernel (a copy-pipeline wait that gave up; never in a correct
- * run) is reported as VG_ECUDA by a later vg_apply on the handle, once the error word's copy has
- * reached the host, or by the next vg_solve.
+ * run) sets an error word in mapped host memory and is reported as VG_ECUDA by the next vg_apply
+ * on the handle after that kernel has finished, or by the next vg_solve; no call adds a check to
+ * the caller's stream.
  * Replaces MixedGpu::apply (vem/CurvedVEM_Darcy_gpu/src/equation_gpu.cu:580-598). */
 int vg_apply(vg_handle* h, const void* x, void* y, int precision, int constrained, void* stream);
 

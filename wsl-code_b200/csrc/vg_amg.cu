@@ -281,6 +281,46 @@ __device__ __forceinline__ T sell_dot(const DevSell<T>& M, int r, X xv) {
     return acc;
 }
 
+// the first SELL_PRE entries of a row (columns, values and, for the pre-smoother, the diagonal at
+// the column) loaded before the programmatic-launch wait: the matrix and its diagonal are written
+// only at set-up and refresh, never by a kernel of the cycle
+constexpr int SELL_PRE = 8;
+template <typename T, bool D>
+struct SellRow {
+    int c[SELL_PRE];
+    T v[SELL_PRE];
+    T d[D ? SELL_PRE : 1];
+    int w = 0;
+    long long o = 0;
+};
+
+template <typename T, bool D>
+__device__ __forceinline__ void sell_fetch(const DevSell<T>& M, int r, const T* dinv, SellRow<T, D>& R) {
+    const int s = r >> 5, l = r & 31;
+    R.o = __ldg(M.soff + s) + l;
+    R.w = __ldg(M.width + s);
+#pragma unroll
+    for (int k = 0; k < SELL_PRE; ++k) {
+        R.c[k] = k < R.w ? __ldg(M.col + R.o + 32 * k) : 0;
+        R.v[k] = k < R.w ? __ldg(M.val + R.o + 32 * k) : T(0);
+    }
+    if constexpr (D) {
+#pragma unroll
+        for (int k = 0; k < SELL_PRE; ++k) R.d[k] = k < R.w ? __ldg(dinv + R.c[k]) : T(0);
+    }
+}
+
+// sum_k val_k xv(k, col_k) in the order of sell_dot (the same result, bit for bit)
+template <typename T, bool D, class X>
+__device__ __forceinline__ T sell_finish(const DevSell<T>& M, const SellRow<T, D>& R, X xv) {
+    T acc = T(0);
+#pragma unroll
+    for (int k = 0; k < SELL_PRE; ++k)
+        if (k < R.w) acc += R.v[k] * xv(k, R.c[k]);
+    for (int k = SELL_PRE; k < R.w; ++k) acc += __ldg(M.val + R.o + 32 * k) * xv(-1, __ldg(M.col + R.o + 32 * k));
+    return acc;
+}
+
 template <typename T>
 __device__ __forceinline__ T sell_row(const DevSell<T>& M, int r, const T* x) {
     return sell_dot(M, r, [&](int c) { return x[c]; });
@@ -297,14 +337,19 @@ template <typename T>
 __global__ void __launch_bounds__(TPB) k_jacobi0_residual(DevSell<T> A, const T* dinv, T omega, const T* b, T* t,
                                                           T* r) {
     pdl_trigger();
+    const int i = blockIdx.x * TPB + threadIdx.x;
+    SellRow<T, true> R;
+    if (i < A.n) sell_fetch<T, true>(A, i, dinv, R);
+    const T di = i < A.n ? __ldg(dinv + i) : T(0);
     pdl_wait();
-    int i = blockIdx.x * TPB + threadIdx.x;
     if (i >= A.n) return;
     // vectors written by earlier kernels of the cycle are read with plain loads after the wait
     // (never ld.global.nc, which the compiler may move above it)
-    const T acc = sell_dot(A, i, [&](int c) { return omega * __ldg(dinv + c) * b[c]; });
+    const T acc = sell_finish<T, true>(A, R, [&](int k, int c) {
+        return omega * (k >= 0 ? R.d[k < 0 ? 0 : k] : __ldg(dinv + c)) * b[c];
+    });
     const T bi = b[i];
-    t[i] = omega * dinv[i] * bi;
+    t[i] = omega * di * bi;
     r[i] = bi - acc;
 }
 
@@ -329,10 +374,13 @@ __global__ void __launch_bounds__(TPB) k_prolong_add(DevSell<T> P, const T* xc, 
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_smooth(DevSell<T> A, const T* dinv, T omega, const T* b, const T* x, T* xo) {
     pdl_trigger();
+    const int i = blockIdx.x * TPB + threadIdx.x;
+    SellRow<T, false> R;
+    if (i < A.n) sell_fetch<T, false>(A, i, nullptr, R);
+    const T di = i < A.n ? __ldg(dinv + i) : T(0);
     pdl_wait();
-    int i = blockIdx.x * TPB + threadIdx.x;
     if (i < A.n)
-        xo[i] = x[i] + omega * dinv[i] * (b[i] - sell_dot(A, i, [&](int c) { return x[c]; }));
+        xo[i] = x[i] + omega * di * (b[i] - sell_finish<T, false>(A, R, [&](int, int c) { return x[c]; }));
 }
 
 // ---- CSR in row blocks (the CSR-stream scheme of Greathouse and Daga, SC 2014, with the entries

@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
             issued_sh = issued;
             if (!ok) {
                 abort_flag = 1;
-                atomicExch(a.err, 1);
+                *reinterpret_cast<volatile int*>(a.err) = 1;
             }
         }
     } else {  // consumers
@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
             if (!ok) {
                 if (lane == 0) {
                     abort_flag = 1;
-                    atomicExch(a.err, 1);
+                    *reinterpret_cast<volatile int*>(a.err) = 1;
                 }
                 break;
             }

@@ -202,7 +202,6 @@ int vg_apply(vg_handle* h, const void* x, void* y, int precision, int constraine
         } else {
             throw vg::Error(VG_EINVAL, "precision must be VG_FP64 or VG_FP32");
         }
-        s.probe_apply_error(st);
     });
 }
 

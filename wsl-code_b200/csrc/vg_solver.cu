@@ -288,12 +288,6 @@ Solver::Solver(HostMesh&& mesh, const vg_geometry* geo, int k_, int nq_, int ng_
 Solver::~Solver() {
     destroy_graphs();
     ms_destroy_graphs();
-    if (probe_) {
-        cudaStreamSynchronize(probe_);
-        cudaStreamDestroy(probe_);
-    }
-    if (ev_applied_) cudaEventDestroy(ev_applied_);
-    if (ev_probed_) cudaEventDestroy(ev_probed_);
     if (h_err_) cudaFreeHost(h_err_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
@@ -936,8 +930,13 @@ void Solver::plan_streams() {
     d_bat32_.upload(plan32_.batches);
     d_cta64_.upload(plan64_.cta_batch);
     d_cta32_.upload(plan32_.cta_batch);
-    d_err_.resize(1);
-    d_err_.zero();
+    // the apply's error word: mapped pinned host memory, written by a kernel only when a pipeline
+    // wait gave up (a plain store) and read by the host with a plain load, no copy in any call
+    if (!h_err_) {
+        VG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h_err_), sizeof(int), cudaHostAllocMapped));
+        *h_err_ = 0;
+        VG_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&d_errp_), h_err_, 0));
+    }
     d_stall_.resize(1);
     d_stall_.zero();
     VG_CUDA(cudaDeviceSynchronize());
@@ -963,37 +962,13 @@ void Solver::inject_apply_stall() {
     VG_CUDA(cudaMemcpy(d_stall_.data(), &one, sizeof(one), cudaMemcpyHostToDevice));
 }
 
-// vg_apply is asynchronous: after its kernel, a copy of the error word is queued on a private
-// stream (ordered after the caller's stream by an event) into pinned host memory. The next call
-// on the handle looks at the copy if it has completed and reports a failed apply as VG_ECUDA;
-// the caller's stream never waits for it.
-void Solver::probe_apply_error(cudaStream_t s) {
-    if (k > 1 || !d_err_.data()) return;
-    if (!probe_) {
-        VG_CUDA(cudaStreamCreateWithFlags(&probe_, cudaStreamNonBlocking));
-        VG_CUDA(cudaEventCreateWithFlags(&ev_applied_, cudaEventDisableTiming));
-        VG_CUDA(cudaEventCreateWithFlags(&ev_probed_, cudaEventDisableTiming));
-        VG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h_err_), sizeof(int), cudaHostAllocDefault));
-        *h_err_ = 0;
-    }
-    VG_CUDA(cudaEventRecord(ev_applied_, s));
-    VG_CUDA(cudaStreamWaitEvent(probe_, ev_applied_, 0));
-    VG_CUDA(cudaMemcpyAsync(h_err_, d_err_.data(), sizeof(int), cudaMemcpyDeviceToHost, probe_));
-    VG_CUDA(cudaEventRecord(ev_probed_, probe_));
-    probe_pending_ = true;
-}
-
+// vg_apply is asynchronous: a failed apply sets the mapped error word when its kernel gives up,
+// and the next call on the handle that finds it set reports VG_ECUDA (the caller's stream never
+// waits for a check)
 void Solver::check_apply_probe() {
-    if (!probe_pending_) return;
-    const cudaError_t q = cudaEventQuery(ev_probed_);
-    if (q == cudaErrorNotReady) return;
-    VG_CUDA(q);
-    probe_pending_ = false;
-    if (*h_err_) {
-        *h_err_ = 0;
+    if (h_err_ && *reinterpret_cast<volatile int*>(h_err_)) {
         VG_CUDA(cudaDeviceSynchronize());
-        d_err_.zero();
-        VG_CUDA(cudaDeviceSynchronize());
+        *reinterpret_cast<volatile int*>(h_err_) = 0;
         throw Error(VG_ECUDA, "an earlier vg_apply failed: apply pipeline wait timed out");
     }
 }
@@ -1002,16 +977,9 @@ void Solver::check_apply_probe() {
 void Solver::check_pipeline() {
     if (amg_.ready() && amg_.failed()) throw Error(VG_ECUDA, "multigrid copy wait timed out");
     if (k > 1) return;
-    int e = 0;
-    VG_CUDA(cudaMemcpy(&e, d_err_.data(), sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) {
-        d_err_.zero();
+    if (h_err_ && *reinterpret_cast<volatile int*>(h_err_)) {
         VG_CUDA(cudaDeviceSynchronize());
-        if (probe_pending_) {  // the same failure is not reported twice
-            VG_CUDA(cudaStreamSynchronize(probe_));
-            *h_err_ = 0;
-            probe_pending_ = false;
-        }
+        *reinterpret_cast<volatile int*>(h_err_) = 0;
         throw Error(VG_ECUDA, "apply pipeline wait timed out");
     }
 }
@@ -1061,7 +1029,7 @@ ApplyArgs<T> Solver::apply_args(const T* x, T* y, bool constrained, T psign, dou
     a.partials = d_partials_.data();
     a.counter = d_counter_.data();
     a.red = quad;
-    if (k <= 1 && d_err_.data()) {
+    if (k <= 1 && d_errp_) {
         const StreamPlan& pl = sizeof(T) == 8 ? plan64_ : plan32_;
         a.rec = sizeof(T) == 8 ? d_rec64_.data() : d_rec32_.data();
         a.batches = sizeof(T) == 8 ? d_bat64_.data() : d_bat32_.data();
@@ -1069,7 +1037,7 @@ ApplyArgs<T> Solver::apply_args(const T* x, T* y, bool constrained, T psign, dou
         a.ncta = pl.ncta;
         a.stages = pl.stages;
         a.stage_bytes = pl.stage_bytes;
-        a.err = d_err_.data();
+        a.err = d_errp_;
         a.stall = d_stall_.data();
     }
     return a;

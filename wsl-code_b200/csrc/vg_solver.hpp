@@ -73,7 +73,6 @@ public:
     int device() const { return device_; }  // the CUDA device that holds this handle's data
     // failure-path test hook and the asynchronous error report of vg_apply
     void inject_apply_stall();
-    void probe_apply_error(cudaStream_t s);
     void check_apply_probe();
     void cell_areas(double* out);
     // assembled CSR of the system (comparator of the matrix-free apply); rp == nullptr: size only
@@ -228,12 +227,9 @@ private:
     DevBuf<long long> d_roff64_, d_roff32_;
     DevBuf<ApplyBatch> d_bat64_, d_bat32_;
     DevBuf<int> d_cta64_, d_cta32_;
-    DevBuf<int> d_err_;
-    DevBuf<int> d_stall_;  // test hook of the streamed apply (zero in every normal run)
-    cudaStream_t probe_ = nullptr;
-    cudaEvent_t ev_applied_ = nullptr, ev_probed_ = nullptr;
-    int* h_err_ = nullptr;  // pinned copy of d_err_ after the last vg_apply
-    bool probe_pending_ = false;
+    int* h_err_ = nullptr;   // the apply's error word (mapped pinned host memory) ...
+    int* d_errp_ = nullptr;  // ... and its device address
+    DevBuf<int> d_stall_;    // test hook of the streamed apply (zero in every normal run)
     DevBuf<double> d_hb_, d_hx_;  // device copies of the host-buffer solve
     DevBuf<double> d_rhs0_;       // right-hand side before the essential-BC lift
     DevBuf<double> d_adj_rhs_, d_adj_mu_;  // adjoint right-hand side and solution
