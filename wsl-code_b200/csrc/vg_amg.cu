@@ -233,6 +233,30 @@ HostCsr smoothed_prolongator(const HostCsr& A, const std::vector<int>& agg, int 
     return P;
 }
 
+// Pt = (I - omega D^{-1} A) P from P and the product A P: the union of their row patterns, no entry
+// dropped (the pattern stays valid for the values of a refresh)
+HostCsr transfer_smooth(const HostCsr& P, const HostCsr& AP, const std::vector<double>& dinv, double omega) {
+    HostCsr Q;
+    Q.n = P.n;
+    Q.m = P.m;
+    Q.ptr.assign(P.n + 1, 0);
+    for (int i = 0; i < P.n; ++i) {
+        const double f = omega * dinv[i];
+        int a = P.ptr[i], b = AP.ptr[i];
+        const int ae = P.ptr[i + 1], be = AP.ptr[i + 1];
+        while (a < ae || b < be) {
+            const int ca = a < ae ? P.col[a] : P.m, cb = b < be ? AP.col[b] : P.m;
+            const int c = std::min(ca, cb);
+            const double pv = ca == c ? P.val[a++] : 0.0;
+            const double apv = cb == c ? AP.val[b++] : 0.0;
+            Q.col.push_back(c);
+            Q.val.push_back(pv - f * apv);
+        }
+        Q.ptr[i + 1] = int(Q.col.size());
+    }
+    return Q;
+}
+
 // dense copy of the coarsest matrix, row-major; a tiny diagonal shift keeps a semi-definite
 // coarsest matrix (constants in the kernel) invertible
 std::vector<double> dense_of(const HostCsr& A) {
@@ -255,47 +279,19 @@ constexpr int TPB = 256;
 constexpr int CSR_CAP = 2048;  // entries staged per CSR row block
 constexpr int CSR_RPT = 4;     // rows per thread of a CSR row block (at most CSR_RPT * TPB rows)
 
-// one row of a SELL-32 matrix: sum_k val_k xv(col_k), entries loaded four at a time before their
-// gathers (independent loads in flight), fixed summation order
-template <typename T, class X>
-__device__ __forceinline__ T sell_dot(const DevSell<T>& M, int r, X xv) {
-    const int s = r >> 5, l = r & 31;
-    const long long o = __ldg(M.soff + s) + l;
-    const int w = __ldg(M.width + s);
-    const int* cp = M.col + o;
-    const T* vp = M.val + o;
-    T acc = T(0);
-    int k = 0;
-    for (; k + 4 <= w; k += 4) {
-        int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * (k + 1)), c2 = __ldg(cp + 32 * (k + 2)),
-            c3 = __ldg(cp + 32 * (k + 3));
-        T v0 = __ldg(vp + 32 * k), v1 = __ldg(vp + 32 * (k + 1)), v2 = __ldg(vp + 32 * (k + 2)),
-          v3 = __ldg(vp + 32 * (k + 3));
-        T x0 = xv(c0), x1 = xv(c1), x2 = xv(c2), x3 = xv(c3);
-        acc += v0 * x0;
-        acc += v1 * x1;
-        acc += v2 * x2;
-        acc += v3 * x3;
-    }
-    for (; k < w; ++k) acc += __ldg(vp + 32 * k) * xv(__ldg(cp + 32 * k));
-    return acc;
-}
-
-// the first SELL_PRE entries of a row (columns, values and, for the pre-smoother, the diagonal at
-// the column) loaded before the programmatic-launch wait: the matrix and its diagonal are written
-// only at set-up and refresh, never by a kernel of the cycle
+// the first SELL_PRE entries of a row (columns and values) loaded before the programmatic-launch
+// wait: the matrix is written only at set-up and refresh, never by a kernel of the cycle
 constexpr int SELL_PRE = 8;
-template <typename T, bool D>
+template <typename T>
 struct SellRow {
     int c[SELL_PRE];
     T v[SELL_PRE];
-    T d[D ? SELL_PRE : 1];
     int w = 0;
     long long o = 0;
 };
 
-template <typename T, bool D>
-__device__ __forceinline__ void sell_fetch(const DevSell<T>& M, int r, const T* dinv, SellRow<T, D>& R) {
+template <typename T>
+__device__ __forceinline__ void sell_fetch(const DevSell<T>& M, int r, SellRow<T>& R) {
     const int s = r >> 5, l = r & 31;
     R.o = __ldg(M.soff + s) + l;
     R.w = __ldg(M.width + s);
@@ -304,83 +300,31 @@ __device__ __forceinline__ void sell_fetch(const DevSell<T>& M, int r, const T* 
         R.c[k] = k < R.w ? __ldg(M.col + R.o + 32 * k) : 0;
         R.v[k] = k < R.w ? __ldg(M.val + R.o + 32 * k) : T(0);
     }
-    if constexpr (D) {
-#pragma unroll
-        for (int k = 0; k < SELL_PRE; ++k) R.d[k] = k < R.w ? __ldg(dinv + R.c[k]) : T(0);
-    }
 }
 
-// sum_k val_k xv(k, col_k) in the order of sell_dot (the same result, bit for bit)
-template <typename T, bool D, class X>
-__device__ __forceinline__ T sell_finish(const DevSell<T>& M, const SellRow<T, D>& R, X xv) {
+// sum_k val_k x(col_k) in entry order (fixed summation order)
+template <typename T>
+__device__ __forceinline__ T sell_finish(const DevSell<T>& M, const SellRow<T>& R, const T* x) {
     T acc = T(0);
 #pragma unroll
     for (int k = 0; k < SELL_PRE; ++k)
-        if (k < R.w) acc += R.v[k] * xv(k, R.c[k]);
-    for (int k = SELL_PRE; k < R.w; ++k) acc += __ldg(M.val + R.o + 32 * k) * xv(-1, __ldg(M.col + R.o + 32 * k));
+        if (k < R.w) acc += R.v[k] * x[R.c[k]];
+    for (int k = SELL_PRE; k < R.w; ++k) acc += __ldg(M.val + R.o + 32 * k) * x[__ldg(M.col + R.o + 32 * k)];
     return acc;
 }
 
+// residual of one Jacobi step from zero, r = b - (A S) b, on the SELL-32 finest level (the stored
+// values are those of A S, so only b is gathered). b is written by an earlier kernel: read with
+// plain loads after the programmatic-launch wait (never ld.global.nc, which the compiler may move
+// above it)
 template <typename T>
-__device__ __forceinline__ T sell_row(const DevSell<T>& M, int r, const T* x) {
-    return sell_dot(M, r, [&](int c) { return x[c]; });
-}
-
-template <typename T>
-__global__ void __launch_bounds__(TPB) k_jacobi0(int n, const T* dinv, T omega, const T* b, T* x) {
-    int i = blockIdx.x * TPB + threadIdx.x;
-    if (i < n) x[i] = omega * dinv[i] * b[i];
-}
-
-// pre-smoothing from zero fused with the residual: t = omega D^{-1} b, r = b - A t
-template <typename T>
-__global__ void __launch_bounds__(TPB) k_jacobi0_residual(DevSell<T> A, const T* dinv, T omega, const T* b, T* t,
-                                                          T* r) {
+__global__ void __launch_bounds__(TPB) k_sell_residual(DevSell<T> A, const T* b, T* r) {
     pdl_trigger();
     const int i = blockIdx.x * TPB + threadIdx.x;
-    SellRow<T, true> R;
-    if (i < A.n) sell_fetch<T, true>(A, i, dinv, R);
-    const T di = i < A.n ? __ldg(dinv + i) : T(0);
+    SellRow<T> R;
+    if (i < A.n) sell_fetch<T>(A, i, R);
     pdl_wait();
-    if (i >= A.n) return;
-    // vectors written by earlier kernels of the cycle are read with plain loads after the wait
-    // (never ld.global.nc, which the compiler may move above it)
-    const T acc = sell_finish<T, true>(A, R, [&](int k, int c) {
-        return omega * (k >= 0 ? R.d[k < 0 ? 0 : k] : __ldg(dinv + c)) * b[c];
-    });
-    const T bi = b[i];
-    t[i] = omega * di * bi;
-    r[i] = bi - acc;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(TPB) k_residual(DevSell<T> A, const T* b, const T* x, T* r) {
-    int i = blockIdx.x * TPB + threadIdx.x;
-    if (i < A.n) r[i] = b[i] - sell_row(A, i, x);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(TPB) k_spmv(DevSell<T> M, const T* x, T* y) {
-    int i = blockIdx.x * TPB + threadIdx.x;
-    if (i < M.n) y[i] = sell_row(M, i, x);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(TPB) k_prolong_add(DevSell<T> P, const T* xc, T* x) {
-    int i = blockIdx.x * TPB + threadIdx.x;
-    if (i < P.n) x[i] += sell_row(P, i, xc);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(TPB) k_smooth(DevSell<T> A, const T* dinv, T omega, const T* b, const T* x, T* xo) {
-    pdl_trigger();
-    const int i = blockIdx.x * TPB + threadIdx.x;
-    SellRow<T, false> R;
-    if (i < A.n) sell_fetch<T, false>(A, i, nullptr, R);
-    const T di = i < A.n ? __ldg(dinv + i) : T(0);
-    pdl_wait();
-    if (i < A.n)
-        xo[i] = x[i] + omega * di * (b[i] - sell_finish<T, false>(A, R, [&](int, int c) { return x[c]; }));
+    if (i < A.n) r[i] = b[i] - sell_finish<T>(A, R, b);
 }
 
 // ---- CSR in row blocks (the CSR-stream scheme of Greathouse and Daga, SC 2014, with the entries
@@ -392,8 +336,8 @@ __global__ void __launch_bounds__(TPB) k_smooth(DevSell<T> A, const T* dinv, T o
 // sums its products in order, so the result does not depend on the launch shape. Vectors written
 // by earlier kernels of the cycle are read with plain loads after the programmatic-launch wait
 // (never ld.global.nc, which the compiler may move above it); the matrix may be read before it.
-// op: 0 y = M x; 1 y += M x (prolongation); 2 smoothing y = x + omega dinv (b - M x);
-//     3 Jacobi from zero with its residual: y = omega dinv b, r = b - M y
+// op: 0 y = M x (restriction); 1 y = omega dinv (b + r) + M x (prolongation with the smoothing
+//     of the composite cycle); 2 y = b - M x (residual, with x = b and M = A S)
 template <typename T>
 struct CsrSmem {
     static constexpr int col_bytes = (CSR_CAP + 8) * 4;
@@ -405,13 +349,8 @@ struct CsrSmem {
 };
 
 template <int OP, typename T>
-__device__ __forceinline__ T csr_x(int c, const T* dinv, T omega, const T* b, const T* x) {
-    if (OP == 3) return omega * __ldg(dinv + c) * b[c];
-    return x[c];
-}
-
-template <int OP, typename T>
-__global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega, const T* b, const T* x, T* y, T* r) {
+__global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega, const T* b, const T* x, T* y,
+                                             const T* r) {
     using L = CsrSmem<T>;
     constexpr int J = CSR_CAP / TPB;
     constexpr int VA = 16 / int(sizeof(T));  // values per 16 bytes
@@ -493,7 +432,7 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
 #pragma unroll
             for (int j = 0; j < J; ++j) {
                 const int k = t + j * TPB;
-                if (k < ne) prod[k] = v[j] * csr_x<OP>(c[j], dinv, omega, b, x);
+                if (k < ne) prod[k] = v[j] * x[c[j]];
             }
             __syncthreads();
 #pragma unroll
@@ -503,7 +442,7 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
         } else if (ne > CSR_CAP) {  // one long row: strided partial sums, fixed-order block reduction
             T part = T(0);
             for (int k = t; k < ne; k += TPB)
-                part += __ldg(M.val + a.y + k) * csr_x<OP>(__ldg(M.col + a.y + k), dinv, omega, b, x);
+                part += __ldg(M.val + a.y + k) * x[__ldg(M.col + a.y + k)];
             for (int off = 16; off; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
             if ((t & 31) == 0) red[t >> 5] = part;
             __syncthreads();
@@ -521,14 +460,9 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
             if (OP == 0)
                 y[row] = acc[q];
             else if (OP == 1)
-                y[row] += acc[q];
-            else if (OP == 2)
-                y[row] = x[row] + omega * dinv[row] * (b[row] - acc[q]);
-            else {
-                const T br = b[row];
-                y[row] = omega * dinv[row] * br;
-                r[row] = br - acc[q];
-            }
+                y[row] = omega * __ldg(dinv + row) * (b[row] + r[row]) + acc[q];
+            else
+                y[row] = b[row] - acc[q];
         }
     }
 }
@@ -547,22 +481,20 @@ void prepare_csr_kernels(int slots[2]) {
     prepare_csr_op<0, float>();
     prepare_csr_op<1, float>();
     prepare_csr_op<2, float>();
-    prepare_csr_op<3, float>();
     prepare_csr_op<0, double>();
     prepare_csr_op<1, double>();
     prepare_csr_op<2, double>();
-    prepare_csr_op<3, double>();
     int dev = 0, n32 = 0, n64 = 0, sms = 0;
     VG_CUDA(cudaGetDevice(&dev));
     VG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n32, k_csr<3, float>, TPB, CsrSmem<float>::total));
-    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n64, k_csr<3, double>, TPB, CsrSmem<double>::total));
+    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n32, k_csr<0, float>, TPB, CsrSmem<float>::total));
+    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n64, k_csr<0, double>, TPB, CsrSmem<double>::total));
     slots[0] = std::max(1, n32) * std::max(1, sms);
     slots[1] = std::max(1, n64) * std::max(1, sms);
 }
 
 template <typename T>
-void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, const T* x, T* y, T* r,
+void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, const T* x, T* y, const T* r,
                 cudaStream_t s) {
     if (M.n <= 0 || M.nblk <= 0) return;
     const int grid = std::min(M.nblk, std::max(1, M.slots));
@@ -570,8 +502,7 @@ void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, 
     switch (op) {
     case 0: launch_pdl(k_csr<0, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
     case 1: launch_pdl(k_csr<1, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
-    case 2: launch_pdl(k_csr<2, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
-    default: launch_pdl(k_csr<3, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
+    default: launch_pdl(k_csr<2, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
     }
 }
 
@@ -746,9 +677,40 @@ __global__ void k_rap(const int* rptr, const int* rcol, const double* rval, cons
     }
 }
 
-__global__ void k_put_sell(const double* csr, const long long* pos, double* sell, long long n) {
-    for (long long i = blockIdx.x * (long long)TPB + threadIdx.x; i < n; i += (long long)gridDim.x * TPB)
-        sell[pos[i]] = csr[i];
+// Pt = (I - omega D^{-1} A) P on Pt's fixed pattern, one row per thread: the products A P of the row
+// summed in the order of the host set-up (A's entries, then P's), then Pt = P - omega d_i (A P)
+__global__ void k_ptilde(const int* aptr, const int* acol, const double* aval, const double* dinv, double omega,
+                         const int* pptr, const int* pcol, const double* pval, const int* qptr, const int* qcol,
+                         double* qval, int n) {
+    int t = blockIdx.x * TPB + threadIdx.x;
+    if (t >= n) return;
+    const int lo = qptr[t], hi = qptr[t + 1];
+    for (int j = lo; j < hi; ++j) qval[j] = 0.0;
+    for (int e = aptr[t]; e < aptr[t + 1]; ++e) {
+        const int k = acol[e];
+        const double a = aval[e];
+        for (int w = pptr[k]; w < pptr[k + 1]; ++w) {
+            const int j = find_col(qcol, lo, hi, pcol[w]);
+            if (j < hi && qcol[j] == pcol[w]) qval[j] += a * pval[w];
+        }
+    }
+    const double f = omega * dinv[t];
+    int w = pptr[t];
+    for (int j = lo; j < hi; ++j) {
+        while (w < pptr[t + 1] && pcol[w] < qcol[j]) ++w;
+        const double pv = (w < pptr[t + 1] && pcol[w] == qcol[j]) ? pval[w] : 0.0;
+        qval[j] = pv - f * qval[j];
+    }
+}
+
+// values of A S (columns scaled by omega D^{-1}) from A's stored CSR values, into CSR (pos null)
+// or SELL slots
+__global__ void k_scale_cols(const double* aval, const int* acol, const double* dinv, double omega,
+                             const long long* pos, double* out, long long n) {
+    for (long long i = blockIdx.x * (long long)TPB + threadIdx.x; i < n; i += (long long)gridDim.x * TPB) {
+        const double v = aval[i] * (omega * dinv[acol[i]]);
+        out[pos ? pos[i] : i] = v;
+    }
 }
 
 __global__ void k_to32(const double* a, float* b, long long n) {
@@ -815,6 +777,17 @@ void Amg::dense_inverse_of(double* dd, int n) {
     if (b) throw Error(VG_ESINGULAR, "coarsest multigrid matrix is not positive definite");
 }
 
+Amg::~Amg() { release_streams(); }
+
+void Amg::release_streams() {
+    for (cudaEvent_t e : ev_fork_) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_join_) cudaEventDestroy(e);
+    ev_fork_.clear();
+    ev_join_.clear();
+    if (side_) cudaStreamDestroy(side_);
+    side_ = nullptr;
+}
+
 void Amg::refresh(const double* a0) {
     if (levels_.empty()) throw Error(VG_ESTATE, "multigrid refresh before setup");
     PhaseTimer pt;
@@ -823,14 +796,6 @@ void Amg::refresh(const double* a0) {
     for (int l = 0; l < nl; ++l) {
         Level& L = levels_[l];
         const long long nnz = (long long)L.pa_col.size();
-        if (L.A.csr) {
-            if (aval != L.cA_v64.data())
-                VG_CUDA(cudaMemcpy(L.cA_v64.data(), aval, sizeof(double) * nnz, cudaMemcpyDeviceToDevice));
-            k_to32<<<148 * 4, TPB>>>(L.cA_v64.data(), L.cA_v32.data(), nnz);
-        } else {
-            k_put_sell<<<148 * 4, TPB>>>(aval, L.dsellpos.data(), L.dA_v64.data(), nnz);
-            k_to32<<<148 * 4, TPB>>>(L.dA_v64.data(), L.dA_v32.data(), (long long)L.dA_v64.size());
-        }
         k_diag_inv<<<blocks(L.n), TPB>>>(L.dpa_ptr.data(), L.dpa_col.data(), aval, L.n, L.dinv64.data(),
                                          L.dinv32.data());
         VG_CUDA(cudaGetLastError());
@@ -845,35 +810,120 @@ void Amg::refresh(const double* a0) {
             pt.mark("refresh: coarsest inverse");
             break;
         }
-        const long long pn = (long long)L.P.ccol.size(), rn = (long long)L.R.ccol.size();
+        // A S for the residual
+        if (L.A.csr) {
+            k_scale_cols<<<148 * 4, TPB>>>(aval, L.dpa_col.data(), L.dinv64.data(), L.omega, nullptr, L.cA.v64.data(),
+                                           nnz);
+            k_to32<<<148 * 4, TPB>>>(L.cA.v64.data(), L.cA.v32.data(), nnz);
+        } else {
+            k_scale_cols<<<148 * 4, TPB>>>(aval, L.dpa_col.data(), L.dinv64.data(), L.omega, L.dsellpos.data(),
+                                           L.dA_v64.data(), nnz);
+            k_to32<<<148 * 4, TPB>>>(L.dA_v64.data(), L.dA_v32.data(), (long long)L.dA_v64.size());
+        }
+        // P, R = P^T (FP64: the next level's Galerkin product), Pt = (I - S A) P and Rt = Pt^T
         if (!L.fixedP)
             k_smooth_p<<<blocks(L.n), TPB>>>(L.dpa_ptr.data(), L.dpa_col.data(), aval, L.dagg.data(), L.dinv64.data(),
-                                             L.omega, L.cP_ptr.data(), L.cP_col.data(), L.cP_v64.data(), L.n);
-        k_take<<<148 * 4, TPB>>>(L.cP_v64.data(), L.dr2p.data(), L.cR_v64.data(), rn);
-        k_to32<<<148 * 4, TPB>>>(L.cP_v64.data(), L.cP_v32.data(), pn);
-        k_to32<<<148 * 4, TPB>>>(L.cR_v64.data(), L.cR_v32.data(), rn);
+                                             L.omega, L.cP.ptr.data(), L.cP.col.data(), L.cP.v64.data(), L.n);
+        k_take<<<148 * 4, TPB>>>(L.cP.v64.data(), L.dr2p.data(), L.cR.v64.data(), (long long)L.r2p.size());
+        k_ptilde<<<blocks(L.n), TPB>>>(L.dpa_ptr.data(), L.dpa_col.data(), aval, L.dinv64.data(), L.omega,
+                                       L.cP.ptr.data(), L.cP.col.data(), L.cP.v64.data(), L.cPt.ptr.data(),
+                                       L.cPt.col.data(), L.cPt.v64.data(), L.n);
+        const long long ptn = (long long)L.rt2pt.size();
+        k_take<<<148 * 4, TPB>>>(L.cPt.v64.data(), L.drt2pt.data(), L.cRt.v64.data(), ptn);
+        k_to32<<<148 * 4, TPB>>>(L.cPt.v64.data(), L.cPt.v32.data(), ptn);
+        k_to32<<<148 * 4, TPB>>>(L.cRt.v64.data(), L.cRt.v32.data(), ptn);
         Level& C = levels_[l + 1];
-        if (!C.A.csr) throw Error(VG_ESTATE, "multigrid refresh: coarse operator not in CSR storage");
-        k_rap<<<blocks(L.nc), TPB>>>(L.cR_ptr.data(), L.cR_col.data(), L.cR_v64.data(), L.dpa_ptr.data(),
-                                      L.dpa_col.data(), aval, L.cP_ptr.data(), L.cP_col.data(), L.cP_v64.data(),
-                                      C.cA_ptr.data(), C.cA_col.data(), C.cA_v64.data(), L.nc);
+        k_rap<<<blocks(L.nc), TPB>>>(L.cR.ptr.data(), L.cR.col.data(), L.cR.v64.data(), L.dpa_ptr.data(),
+                                      L.dpa_col.data(), aval, L.cP.ptr.data(), L.cP.col.data(), L.cP.v64.data(),
+                                      C.dpa_ptr.data(), C.dpa_col.data(), C.dvals.data(), L.nc);
         VG_CUDA(cudaGetLastError());
-        aval = C.cA_v64.data();
+        aval = C.dvals.data();
     }
     VG_CUDA(cudaDeviceSynchronize());
 }
 
 long long Amg::nnz() const {
     long long t = 0;
-    for (const auto& L : levels_) t += (long long)(L.A.csr ? L.A.ccol.size() : L.A.col.size());
+    for (const auto& L : levels_) t += (long long)L.pa_col.size();
     return t;
 }
 
 void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int>* fine_order) {
     PhaseTimer pt;
     levels_.clear();
+    release_streams();
     HostCsr A = S0;
     const double theta = 0.08;
+    // storage: SELL-32 (one thread per row) only for the regular fine-level operator; every other
+    // matrix (rectangular transfers, the denser coarse operators) as CSR in row blocks (k_csr)
+    auto to_sell = [&](const HostCsr& M, Sell& S, bool sell_ok) {
+        S.n = M.n;
+        double avg = M.n ? double(M.col.size()) / M.n : 0.0;
+        if (!(sell_ok && avg <= 10.0)) {
+            S.csr = true;
+            S.cptr = M.ptr;
+            S.ccol = M.col;
+            S.cval = M.val;
+            S.nslices = 0;
+            // row blocks: at most CSR_RPT * TPB rows and about nnz / (4 blocks per SM) entries,
+            // between 256 and CSR_CAP (a longer single row is a block of its own)
+            const long long nnz = (long long)M.col.size();
+            const int cap = int(std::min<long long>(CSR_CAP, std::max<long long>(256, (nnz + 591) / 592)));
+            S.rb.assign({0, 0});
+            for (int r = 0; r < M.n;) {
+                const int start = r;
+                long long nn = 0;
+                while (r < M.n && r - start < CSR_RPT * TPB) {
+                    const int len = M.ptr[r + 1] - M.ptr[r];
+                    if (r > start && nn + len > cap) break;
+                    nn += len;
+                    ++r;
+                }
+                S.rb.push_back(r);
+                S.rb.push_back(M.ptr[r]);
+            }
+            return;
+        }
+        S.nslices = (M.n + 31) / 32;
+        S.soff.assign(S.nslices + 1, 0);
+        S.width.assign(S.nslices, 0);
+        for (int s = 0; s < S.nslices; ++s) {
+            int w = 0;
+            for (int r = s * 32; r < std::min(M.n, s * 32 + 32); ++r) w = std::max(w, M.ptr[r + 1] - M.ptr[r]);
+            S.width[s] = w;
+            S.soff[s + 1] = S.soff[s] + 32LL * w;
+        }
+        S.col.assign(S.soff[S.nslices], 0);
+        S.val.assign(S.soff[S.nslices], 0.0);
+        for (int s = 0; s < S.nslices; ++s)
+            for (int l = 0; l < 32; ++l) {
+                int r = s * 32 + l;
+                for (int k = 0; k < S.width[s]; ++k) {
+                    long long o = S.soff[s] + 32LL * k + l;
+                    if (r < M.n && k < M.ptr[r + 1] - M.ptr[r]) {
+                        S.col[o] = M.col[M.ptr[r] + k];
+                        S.val[o] = M.val[M.ptr[r] + k];
+                    } else {
+                        S.col[o] = 0;  // padding reads column 0 with value 0
+                        S.val[o] = 0.0;
+                    }
+                }
+            }
+    };
+    // CSR on the device (row blocks; column and value arrays padded by 4 entries: k_csr copies
+    // 16-byte aligned supersets of each block's ranges)
+    auto upload_csr = [](const Sell& S, CsrBufs& B) {
+        B.rb.upload(S.rb);
+        B.ptr.upload(S.cptr);
+        std::vector<int> cc(S.ccol);
+        cc.resize(cc.size() + 4, 0);
+        B.col.upload(cc);
+        std::vector<double> vv(S.cval);
+        vv.resize(vv.size() + 4, 0.0);
+        B.v64.upload(vv);
+        std::vector<float> f(vv.begin(), vv.end());
+        B.v32.upload(f);
+    };
     while (true) {
         Level L;
         L.n = A.n;
@@ -882,116 +932,74 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
             double d = diag_of(A, i);
             L.dinv[i] = d != 0.0 ? 1.0 / d : 0.0;
         }
-        // storage: SELL-32 (one thread per row) only for the regular fine-level operator; every other
-        // matrix (rectangular P and R, the denser coarse operators) as CSR in row blocks (k_csr)
-        auto to_sell = [&](const HostCsr& M, Sell& S, bool sell_ok) {
-            S.n = M.n;
-            double avg = M.n ? double(M.col.size()) / M.n : 0.0;
-            if (!(sell_ok && avg <= 10.0)) {
-                S.csr = true;
-                S.cptr = M.ptr;
-                S.ccol = M.col;
-                S.cval = M.val;
-                S.nslices = 0;
-                // row blocks: at most CSR_RPT * TPB rows and about nnz / (4 blocks per SM) entries,
-                // between 256 and CSR_CAP (a longer single row is a block of its own)
-                const long long nnz = (long long)M.col.size();
-                const int cap = int(std::min<long long>(CSR_CAP, std::max<long long>(256, (nnz + 591) / 592)));
-                S.rb.assign({0, 0});
-                for (int r = 0; r < M.n;) {
-                    const int start = r;
-                    long long nn = 0;
-                    while (r < M.n && r - start < CSR_RPT * TPB) {
-                        const int len = M.ptr[r + 1] - M.ptr[r];
-                        if (r > start && nn + len > cap) break;
-                        nn += len;
-                        ++r;
-                    }
-                    S.rb.push_back(r);
-                    S.rb.push_back(M.ptr[r]);
-                }
-                return;
-            }
-            S.nslices = (M.n + 31) / 32;
-            S.soff.assign(S.nslices + 1, 0);
-            S.width.assign(S.nslices, 0);
-            for (int s = 0; s < S.nslices; ++s) {
-                int w = 0;
-                for (int r = s * 32; r < std::min(M.n, s * 32 + 32); ++r) w = std::max(w, M.ptr[r + 1] - M.ptr[r]);
-                S.width[s] = w;
-                S.soff[s + 1] = S.soff[s] + 32LL * w;
-            }
-            S.col.assign(S.soff[S.nslices], 0);
-            S.val.assign(S.soff[S.nslices], 0.0);
-            for (int s = 0; s < S.nslices; ++s)
-                for (int l = 0; l < 32; ++l) {
-                    int r = s * 32 + l;
-                    for (int k = 0; k < S.width[s]; ++k) {
-                        long long o = S.soff[s] + 32LL * k + l;
-                        if (r < M.n && k < M.ptr[r + 1] - M.ptr[r]) {
-                            S.col[o] = M.col[M.ptr[r] + k];
-                            S.val[o] = M.val[M.ptr[r] + k];
-                        } else {
-                            // padding reads column 0, which every matrix has (P and R are rectangular:
-                            // the row index is not a valid column)
-                            S.col[o] = 0;
-                            S.val[o] = 0.0;
-                        }
-                    }
-                }
-        };
         // the finest level is coarsened in the given matrix's order (aggregation visits rows in
         // order) and stored in fine_order, the order of the vectors it will act on
         const bool fine = levels_.empty() && fine_order;
         const std::vector<double> dinv_own(L.dinv);  // in A's own order (smoothing, spectral radius)
-        {
-            HostCsr Ast = fine ? permute_csr(A, fine_order, fine_order) : A;
-            if (fine)
-                for (int i = 0; i < A.n; ++i) L.dinv[(*fine_order)[i]] = dinv_own[i];
-            to_sell(Ast, L.A, levels_.empty());
-            L.pa_ptr = Ast.ptr;
-            L.pa_col = Ast.col;
-            if (!L.A.csr) {
-                L.sellpos.resize(Ast.col.size());
-                for (int r = 0; r < Ast.n; ++r)
-                    for (int j = Ast.ptr[r]; j < Ast.ptr[r + 1]; ++j)
-                        L.sellpos[j] = L.A.soff[r / 32] + 32LL * (j - Ast.ptr[r]) + r % 32;
-            }
-        }
-        if (A.n <= COARSE_MAX || levels_.size() >= 16) {
-            if (fine) A = permute_csr(A, fine_order, fine_order);
-            levels_.push_back(std::move(L));
-            break;
-        }
+        if (fine)
+            for (int i = 0; i < A.n; ++i) L.dinv[(*fine_order)[i]] = dinv_own[i];
+        // prolongator (smoothed aggregation, or the given one on the finest level)
         HostCsr P;
         int nagg = 0;
-        if (levels_.empty() && first_P) {
+        bool last = A.n <= COARSE_MAX || levels_.size() >= 16;
+        if (!last && levels_.empty() && first_P) {
             if (first_P->n != A.n || first_P->m <= 0 || first_P->m >= A.n)
                 throw Error(VG_EINVAL, "first multigrid prolongator does not fit the matrix");
             L.omega = 4.0 / (3.0 * rho_dinv_a(A, dinv_own));
             P = *first_P;
             nagg = P.m;
             L.fixedP = true;
-        } else {
+        } else if (!last) {
             std::vector<int> agg = aggregate(A, theta, nagg);
-            if (nagg >= A.n || nagg == 0) {  // no coarsening possible
-                if (fine) A = permute_csr(A, fine_order, fine_order);
-                levels_.push_back(std::move(L));
-                break;
+            if (nagg >= A.n || nagg == 0) {
+                last = true;  // no coarsening possible
+            } else {
+                L.omega = 4.0 / (3.0 * rho_dinv_a(A, dinv_own));
+                P = smoothed_prolongator(A, agg, nagg, dinv_own, L.omega);
+                L.agg.resize(A.n);
+                for (int i = 0; i < A.n; ++i) L.agg[fine ? (*fine_order)[i] : i] = agg[i];
             }
-            L.omega = 4.0 / (3.0 * rho_dinv_a(A, dinv_own));
-            P = smoothed_prolongator(A, agg, nagg, dinv_own, L.omega);
-            L.agg.resize(A.n);
-            for (int i = 0; i < A.n; ++i) L.agg[fine ? (*fine_order)[i] : i] = agg[i];
+        }
+        // stored operator: A S (columns scaled by omega D^{-1}) on a level with a coarser one; the
+        // coarsest level keeps only its pattern (refresh) and is inverted densely
+        {
+            HostCsr Ast = fine ? permute_csr(A, fine_order, fine_order) : A;
+            L.pa_ptr = Ast.ptr;
+            L.pa_col = Ast.col;
+            if (!last) {
+                for (size_t j = 0; j < Ast.col.size(); ++j) Ast.val[j] *= L.omega * L.dinv[Ast.col[j]];
+                to_sell(Ast, L.A, levels_.empty());
+                if (!L.A.csr) {
+                    L.sellpos.resize(Ast.col.size());
+                    for (int r = 0; r < Ast.n; ++r)
+                        for (int j = Ast.ptr[r]; j < Ast.ptr[r + 1]; ++j)
+                            L.sellpos[j] = L.A.soff[r / 32] + 32LL * (j - Ast.ptr[r]) + r % 32;
+                }
+            }
+        }
+        if (last) {
+            if (fine) A = permute_csr(A, fine_order, fine_order);
+            levels_.push_back(std::move(L));
+            break;
         }
         HostCsr R = transpose(P);
-        HostCsr Ac = spgemm(R, spgemm(A, P));
+        HostCsr AP = spgemm(A, P);
+        HostCsr Ac = spgemm(R, AP);
+        HostCsr Pt = transfer_smooth(P, AP, dinv_own, L.omega);
         L.nc = nagg;
         {
             HostCsr Pst = fine ? permute_csr(P, fine_order, nullptr) : P;
             HostCsr Rst = transpose_map(Pst, L.r2p);
-            to_sell(Pst, L.P, false);
-            to_sell(Rst, L.R, false);
+            L.cP.ptr.upload(Pst.ptr);
+            L.cP.col.upload(Pst.col);
+            L.cP.v64.upload(Pst.val);
+            L.cR.ptr.upload(Rst.ptr);
+            L.cR.col.upload(Rst.col);
+            L.cR.v64.upload(Rst.val);
+            HostCsr Ptst = fine ? permute_csr(Pt, fine_order, nullptr) : Pt;
+            HostCsr Rtst = transpose_map(Ptst, L.rt2pt);
+            to_sell(Ptst, L.Pt, false);
+            to_sell(Rtst, L.Rt, false);
         }
         levels_.push_back(std::move(L));
         A = std::move(Ac);
@@ -1006,103 +1014,94 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
     dense_inverse_device(dense_of(A), A.n);
     pt.mark("coarsest dense inverse");
     if (PhaseTimer::stats_enabled()) {
-        // diagnostics: rows, stored entries and storage of every level (stderr)
-        auto nz = [](const Sell& S) { return (long long)(S.csr ? S.ccol.size() : S.col.size()); };
+        // diagnostics: rows and stored entries of every level (stderr)
         for (size_t l = 0; l < levels_.size(); ++l) {
             const Level& L = levels_[l];
-            std::fprintf(stderr, "amg level %zu: rows %d A %lld (%s) P %lld (%s) R %lld (%s) omega %.3f\n", l, L.n,
-                         nz(L.A), L.A.csr ? "csr" : "sell", nz(L.P), L.P.csr ? "csr" : "sell", nz(L.R),
-                         L.R.csr ? "csr" : "sell", L.omega);
+            std::fprintf(stderr, "amg level %zu: rows %d A %zu (%s) Pt %zu Rt %zu omega %.3f\n", l, L.n,
+                         L.pa_col.size(), L.A.csr ? "csr" : "sell", L.Pt.ccol.size(), L.Rt.ccol.size(), L.omega);
         }
         std::fprintf(stderr, "amg coarsest dense: %d rows\n", ncoarse_);
     }
     // uploads
-    for (auto& L : levels_) {
-        auto up = [](const Sell& S, DevBuf<long long>& so, DevBuf<int>& w, DevBuf<int>& c, DevBuf<double>& v64,
-                     DevBuf<float>& v32) {
-            if (S.n == 0 || S.csr) return;
-            so.upload(S.soff);
-            w.upload(S.width);
-            c.upload(S.col);
-            v64.upload(S.val);
-            std::vector<float> f(S.val.begin(), S.val.end());
-            v32.upload(f);
-        };
-        up(L.A, L.dA_soff, L.dA_w, L.dA_col, L.dA_v64, L.dA_v32);
-        up(L.P, L.dP_soff, L.dP_w, L.dP_col, L.dP_v64, L.dP_v32);
-        up(L.R, L.dR_soff, L.dR_w, L.dR_col, L.dR_v64, L.dR_v32);
-        auto upc = [](const Sell& S, DevBuf<int>& p, DevBuf<int>& c, DevBuf<double>& v64, DevBuf<float>& v32,
-                      DevBuf<int>& rb) {
-            if (S.n == 0 || !S.csr) return;
-            rb.upload(S.rb);
-            p.upload(S.cptr);
-            // column and value arrays padded by 4 entries: k_csr copies 16-byte aligned supersets
-            std::vector<int> cc(S.ccol);
-            cc.resize(cc.size() + 4, 0);
-            c.upload(cc);
-            std::vector<double> vv(S.cval);
-            vv.resize(vv.size() + 4, 0.0);
-            v64.upload(vv);
-            std::vector<float> f(vv.begin(), vv.end());
-            v32.upload(f);
-        };
-        upc(L.A, L.cA_ptr, L.cA_col, L.cA_v64, L.cA_v32, L.cA_rb);
+    for (size_t l = 0; l < levels_.size(); ++l) {
+        Level& L = levels_[l];
+        const bool coarsest = l + 1 == levels_.size();
+        if (!coarsest) {
+            if (L.A.csr) {
+                upload_csr(L.A, L.cA);
+            } else {
+                L.dA_soff.upload(L.A.soff);
+                L.dA_w.upload(L.A.width);
+                L.dA_col.upload(L.A.col);
+                L.dA_v64.upload(L.A.val);
+                std::vector<float> f(L.A.val.begin(), L.A.val.end());
+                L.dA_v32.upload(f);
+            }
+            upload_csr(L.Pt, L.cPt);
+            upload_csr(L.Rt, L.cRt);
+            if (!L.agg.empty()) L.dagg.upload(L.agg);
+            L.dr2p.upload(L.r2p);
+            L.drt2pt.upload(L.rt2pt);
+            if (!L.sellpos.empty()) L.dsellpos.upload(L.sellpos);
+        }
         L.dpa_ptr.upload(L.pa_ptr);
         L.dpa_col.upload(L.pa_col);
-        if (!L.agg.empty()) L.dagg.upload(L.agg);
-        if (!L.r2p.empty()) L.dr2p.upload(L.r2p);
-        if (!L.sellpos.empty()) L.dsellpos.upload(L.sellpos);
-        upc(L.P, L.cP_ptr, L.cP_col, L.cP_v64, L.cP_v32, L.cP_rb);
-        upc(L.R, L.cR_ptr, L.cR_col, L.cR_v64, L.cR_v32, L.cR_rb);
+        if (l > 0) L.dvals.resize(L.pa_col.size());  // written by refresh()
         L.dinv64.upload(L.dinv);
         std::vector<float> f(L.dinv.begin(), L.dinv.end());
         L.dinv32.upload(f);
-        for (auto* b : {&L.x64, &L.b64, &L.r64, &L.t64}) b->resize(L.n);
-        for (auto* b : {&L.x32, &L.b32, &L.r32, &L.t32}) b->resize(L.n);
+        for (auto* b : {&L.x64, &L.b64, &L.r64}) b->resize(L.n);
+        for (auto* b : {&L.x32, &L.b32, &L.r32}) b->resize(L.n);
     }
     err_.resize(1);
     err_.zero();
     prepare_csr_kernels(csr_slots_);
+    VG_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    ev_fork_.assign(levels_.size(), nullptr);
+    ev_join_.assign(levels_.size(), nullptr);
+    for (size_t l = 0; l < levels_.size(); ++l) {
+        VG_CUDA(cudaEventCreateWithFlags(&ev_fork_[l], cudaEventDisableTiming));
+        VG_CUDA(cudaEventCreateWithFlags(&ev_join_[l], cudaEventDisableTiming));
+    }
     pt.mark("multigrid uploads");
 }
 
 template <typename T>
-DevSell<T> Amg::view(const Level& L, int which) const {
+DevSell<T> Amg::view(const Level& L) const {
     DevSell<T> v;
-    const Sell& S = which == 0 ? L.A : which == 1 ? L.P : L.R;
-    v.n = S.n;
-    v.nslices = S.nslices;
-    const DevBuf<long long>& so = which == 0 ? L.dA_soff : which == 1 ? L.dP_soff : L.dR_soff;
-    const DevBuf<int>& w = which == 0 ? L.dA_w : which == 1 ? L.dP_w : L.dR_w;
-    const DevBuf<int>& c = which == 0 ? L.dA_col : which == 1 ? L.dP_col : L.dR_col;
-    v.soff = so.data();
-    v.width = w.data();
-    v.col = c.data();
+    v.n = L.A.n;
+    v.nslices = L.A.nslices;
+    v.soff = L.dA_soff.data();
+    v.width = L.dA_w.data();
+    v.col = L.dA_col.data();
     if constexpr (sizeof(T) == 8)
-        v.val = reinterpret_cast<const T*>((which == 0 ? L.dA_v64 : which == 1 ? L.dP_v64 : L.dR_v64).data());
+        v.val = reinterpret_cast<const T*>(L.dA_v64.data());
     else
-        v.val = reinterpret_cast<const T*>((which == 0 ? L.dA_v32 : which == 1 ? L.dP_v32 : L.dR_v32).data());
+        v.val = reinterpret_cast<const T*>(L.dA_v32.data());
     return v;
 }
 
 template <typename T>
-DevCsr<T> Amg::cview(const Level& L, int which) const {
+DevCsr<T> Amg::cview(const Sell& S, const CsrBufs& B) const {
     DevCsr<T> v;
-    const Sell& S = which == 0 ? L.A : which == 1 ? L.P : L.R;
     v.n = S.n;
     v.nblk = S.csr ? int(S.rb.size() / 2) - 1 : 0;
     v.slots = csr_slots_[sizeof(T) == 8 ? 1 : 0];
     v.err = const_cast<int*>(err_.data());
-    v.rb = reinterpret_cast<const int2*>((which == 0 ? L.cA_rb : which == 1 ? L.cP_rb : L.cR_rb).data());
-    v.ptr = (which == 0 ? L.cA_ptr : which == 1 ? L.cP_ptr : L.cR_ptr).data();
-    v.col = (which == 0 ? L.cA_col : which == 1 ? L.cP_col : L.cR_col).data();
+    v.rb = reinterpret_cast<const int2*>(B.rb.data());
+    v.ptr = B.ptr.data();
+    v.col = B.col.data();
     if constexpr (sizeof(T) == 8)
-        v.val = reinterpret_cast<const T*>((which == 0 ? L.cA_v64 : which == 1 ? L.cP_v64 : L.cR_v64).data());
+        v.val = reinterpret_cast<const T*>(B.v64.data());
     else
-        v.val = reinterpret_cast<const T*>((which == 0 ? L.cA_v32 : which == 1 ? L.cP_v32 : L.cR_v32).data());
+        v.val = reinterpret_cast<const T*>(B.v32.data());
     return v;
 }
 
+// one level of the composite V(1,1) cycle (the same operator as Jacobi pre-smoothing from zero,
+// residual, restriction, coarse correction, prolongation and Jacobi post-smoothing):
+//   side stream:  r = b - (A S) b
+//   this stream:  b_c = Rt b;  x_c = cycle(b_c);  z = S (b + r) + Pt x_c
 template <typename T>
 void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     Level& L = levels_[l];
@@ -1112,7 +1111,6 @@ void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
         else
             return reinterpret_cast<T*>(d32.data());
     };
-    const T* dinv = buf(L.dinv64, L.dinv32);
     if (l == int(levels_.size()) - 1) {
         const T* inv = sizeof(T) == 8 ? reinterpret_cast<const T*>(dinvc64_.data())
                                       : reinterpret_cast<const T*>(dinvc32_.data());
@@ -1121,34 +1119,22 @@ void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
         return;
     }
     Level& C = levels_[l + 1];
-    T* t = buf(L.t64, L.t32);
+    const T* dinv = buf(L.dinv64, L.dinv32);
     T* r = buf(L.r64, L.r32);
     T* bc = buf(C.b64, C.b32);
     T* xc = buf(C.x64, C.x32);
-    const T om = T(L.omega);
-    // pre-smoothing from zero + residual
+    VG_CUDA(cudaEventRecord(ev_fork_[l], s));
+    VG_CUDA(cudaStreamWaitEvent(side_, ev_fork_[l], 0));
     if (L.A.csr)
-        launch_csr<T>(3, cview<T>(L, 0), dinv, om, b, nullptr, t, r, s);
+        launch_csr<T>(2, cview<T>(L.A, L.cA), nullptr, T(0), b, b, r, nullptr, side_);
     else
-        launch_pdl(k_jacobi0_residual<T>, blocks(L.n), TPB, 0, s, view<T>(L, 0), dinv, om, b, t, r);
-    // restriction
-    if (L.R.csr)
-        launch_csr<T>(0, cview<T>(L, 2), nullptr, T(0), nullptr, r, bc, nullptr, s);
-    else
-        k_spmv<T><<<blocks(C.n), TPB, 0, s>>>(view<T>(L, 2), r, bc);
-    launches += 2;
+        launch_pdl(k_sell_residual<T>, blocks(L.n), TPB, 0, side_, view<T>(L), b, r);
+    VG_CUDA(cudaEventRecord(ev_join_[l], side_));
+    launch_csr<T>(0, cview<T>(L.Rt, L.cRt), nullptr, T(0), nullptr, b, bc, nullptr, s);
     cycle<T>(l + 1, bc, xc, s);
-    // prolongation
-    if (L.P.csr)
-        launch_csr<T>(1, cview<T>(L, 1), nullptr, T(0), nullptr, xc, t, nullptr, s);
-    else
-        k_prolong_add<T><<<blocks(L.n), TPB, 0, s>>>(view<T>(L, 1), xc, t);
-    // post-smoothing
-    if (L.A.csr)
-        launch_csr<T>(2, cview<T>(L, 0), dinv, om, b, t, z, nullptr, s);
-    else
-        launch_pdl(k_smooth<T>, blocks(L.n), TPB, 0, s, view<T>(L, 0), dinv, om, b, t, z);
-    launches += 2;
+    VG_CUDA(cudaStreamWaitEvent(s, ev_join_[l], 0));
+    launch_csr<T>(1, cview<T>(L.Pt, L.cPt), dinv, T(L.omega), b, xc, z, r, s);
+    launches += 3;
 }
 
 bool Amg::failed() {

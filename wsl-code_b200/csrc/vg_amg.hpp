@@ -6,6 +6,15 @@
 // which its own notes call weak for large meshes. Here the pressure block of the SPD block-diagonal
 // MINRES preconditioner is one symmetric V-cycle on S (Jacobi pre- and post-smoothing with the same
 // weight, exact coarsest solve), built on the host once per operator and applied on the device.
+//
+// The cycle runs in a composite form with the same operator. With S_l = omega_l D_l^{-1}, one
+// pre-smoothing step from zero, the residual, the restriction, the coarse correction and one
+// post-smoothing step give, level by level,
+//     r = b - A S b,   b_c = Pt^T b,   z = S (b + r) + Pt x_c,   Pt = (I - S A) P,
+// because P^T (I - A S) = ((I - S A) P)^T for a symmetric A. Per level this is two dependent
+// products on the cycle's critical path (the restriction by Pt^T and the prolongation by Pt)
+// instead of four, and the residual, which only the prolongation of the same level reads, runs on
+// a second stream beside the coarser levels.
 #pragma once
 #include <vector>
 
@@ -50,6 +59,10 @@ constexpr int DENSE_MAX = 4096;
 
 class Amg {
 public:
+    Amg() = default;
+    Amg(const Amg&) = delete;
+    Amg& operator=(const Amg&) = delete;
+    ~Amg();
     // build the hierarchy of S (host CSR, symmetric positive definite or semi-definite); first_P, when
     // given, is the prolongator of the finest level (no aggregation there); fine_order, when given,
     // renumbers the finest level's rows for the vectors the cycle acts on (row i -> fine_order[i])
@@ -85,36 +98,46 @@ private:
         std::vector<int> rb;  // row blocks: (first row, first entry) pairs, one past the last block included
         std::vector<double> cval;
     };
+    struct CsrBufs {  // one CSR matrix on the device: row blocks, pattern, FP64 and FP32 values
+        DevBuf<int> ptr, col, rb;
+        DevBuf<double> v64;
+        DevBuf<float> v32;
+    };
     struct Level {
         int n = 0, nc = 0;
         double omega = 0;
-        Sell A, P, R;  // P: n x nc, R = P^T: nc x n (absent on the coarsest level)
+        // A: the level's operator with its columns scaled by S = omega D^{-1} (A S, for the residual
+        // r = b - A S b); Pt = (I - S A) P: n x nc, Rt = Pt^T: nc x n (absent on the coarsest level)
+        Sell A, Pt, Rt;
         std::vector<double> dinv;
         // structure kept for refresh(): stored CSR pattern of A, aggregate of every stored row (empty
-        // when the prolongator is given), position in P of every R entry, SELL slot of every CSR
-        // entry of A (SELL storage)
-        std::vector<int> pa_ptr, pa_col, agg, r2p;
+        // when the prolongator is given), position in P of every R entry and in Pt of every Rt entry,
+        // SELL slot of every CSR entry of A (SELL storage), patterns of P and R = P^T (FP64 values:
+        // the Galerkin product of the next level is R A P)
+        std::vector<int> pa_ptr, pa_col, agg, r2p, rt2pt;
         std::vector<long long> sellpos;
         bool fixedP = false;
-        DevBuf<int> dpa_ptr, dpa_col, dagg, dr2p;
+        DevBuf<int> dpa_ptr, dpa_col, dagg, dr2p, drt2pt;
         DevBuf<long long> dsellpos;
-        // device
-        DevBuf<long long> dA_soff, dP_soff, dR_soff;
-        DevBuf<int> dA_w, dA_col, dP_w, dP_col, dR_w, dR_col;
-        DevBuf<int> cA_ptr, cA_col, cP_ptr, cP_col, cR_ptr, cR_col, cA_rb, cP_rb, cR_rb;
-        DevBuf<double> cA_v64, cP_v64, cR_v64;
-        DevBuf<float> cA_v32, cP_v32, cR_v32;
-        DevBuf<double> dA_v64, dP_v64, dR_v64, dinv64, x64, b64, r64, t64;
-        DevBuf<float> dA_v32, dP_v32, dR_v32, dinv32, x32, b32, r32, t32;
+        DevBuf<double> dvals;  // unscaled stored values of A (levels below the finest; refresh)
+        CsrBufs cP, cR;        // P and R (FP64 values only; refresh)
+        // device storage of the cycle's matrices
+        DevBuf<long long> dA_soff;
+        DevBuf<int> dA_w, dA_col;
+        DevBuf<double> dA_v64;
+        DevBuf<float> dA_v32;
+        CsrBufs cA, cPt, cRt;
+        DevBuf<double> dinv64, x64, b64, r64;
+        DevBuf<float> dinv32, x32, b32, r32;
     };
     template <typename T>
     void cycle(int l, const T* b, T* z, cudaStream_t s);
     void dense_inverse_device(const std::vector<double>& a, int n);
     void dense_inverse_of(double* d, int n);  // in-place device matrix -> dinvc64_ / dinvc32_
     template <typename T>
-    DevSell<T> view(const Level& L, int which) const;
+    DevSell<T> view(const Level& L) const;
     template <typename T>
-    DevCsr<T> cview(const Level& L, int which) const;
+    DevCsr<T> cview(const Sell& S, const CsrBufs& B) const;
 
     std::vector<Level> levels_;
     int ncoarse_ = 0;
@@ -122,6 +145,11 @@ private:
     int csr_slots_[2] = {1, 1};  // resident CTAs of the CSR kernels on this hierarchy's device (FP32, FP64)
     DevBuf<double> dinvc64_;  // dense inverse of the coarsest matrix
     DevBuf<float> dinvc32_;
+    // second stream of the cycle (the residuals) and, per level, the events that fork it after the
+    // level's right-hand side is written and join it before the level's prolongation
+    cudaStream_t side_ = nullptr;
+    std::vector<cudaEvent_t> ev_fork_, ev_join_;
+    void release_streams();
 };
 
 }  // namespace vg

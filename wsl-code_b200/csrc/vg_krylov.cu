@@ -12,6 +12,7 @@
 // fixed-shape two-level sum (block partials, last block sums them in order): results are
 // bitwise reproducible.
 #include "vg_krylov.cuh"
+#include "vg_pipe.cuh"
 
 namespace vg {
 
@@ -182,6 +183,9 @@ template <typename T>
 __global__ void __launch_bounds__(VEC_THREADS) k_update(MinresVecs<T> v, long long lo, long long hi, Scalars* sc,
                                                         int* flags, double* partials, unsigned* counter,
                                                         long long plo, long long phi, int reduce) {
+    // the first V-cycle kernel after this one (launched with programmatic dependent launch) may
+    // start now and copy its matrix rows while the update runs; it waits for the update's results
+    pdl_trigger();
     if (flags[0]) {
         if (reduce && blockIdx.x == 0 && threadIdx.x == 0) flags[1] = 0;
         return;
