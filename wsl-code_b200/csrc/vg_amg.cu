@@ -387,13 +387,19 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
         const int ne = z.y - a.y;
         const bool staged = ne > 0 && ne <= CSR_CAP;
         int lo[CSR_RPT], hi[CSR_RPT];
+        T ep[CSR_RPT];  // the epilogue's vector operands, loaded before the gathers (independent of them)
 #pragma unroll
         for (int q = 0; q < CSR_RPT; ++q) {
             const int row = a.x + t + q * TPB;
             lo[q] = hi[q] = 0;
+            ep[q] = T(0);
             if (row < z.x) {
                 lo[q] = __ldg(M.ptr + row) - a.y;
                 hi[q] = __ldg(M.ptr + row + 1) - a.y;
+                if (OP == 1)
+                    ep[q] = omega * __ldg(dinv + row) * (b[row] + r[row]);
+                else if (OP == 2)
+                    ep[q] = b[row];
             }
         }
         int c[J];
@@ -460,9 +466,9 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
             if (OP == 0)
                 y[row] = acc[q];
             else if (OP == 1)
-                y[row] = omega * __ldg(dinv + row) * (b[row] + r[row]) + acc[q];
+                y[row] = ep[q] + acc[q];
             else
-                y[row] = b[row] - acc[q];
+                y[row] = ep[q] - acc[q];
         }
     }
 }
