@@ -50,6 +50,8 @@ struct DevCsr {
     const int* ptr = nullptr;
     const int* col = nullptr;
     const T* val = nullptr;
+    int nwb = 0;                // warp blocks: block w covers rows [wb[w].x, wb[w + 1].x), entries [wb[w].y, wb[w + 1].y)
+    const int2* wb = nullptr;
 };
 
 // coarsest level: at most this many rows, inverted densely (2500^2 doubles = 50 MB)
@@ -96,10 +98,11 @@ private:
         bool csr = false;
         std::vector<int> cptr, ccol;
         std::vector<int> rb;  // row blocks: (first row, first entry) pairs, one past the last block included
+        std::vector<int> wb;  // warp blocks (at most 32 rows and WS_CAP entries), same layout
         std::vector<double> cval;
     };
     struct CsrBufs {  // one CSR matrix on the device: row blocks, pattern, FP64 and FP32 values
-        DevBuf<int> ptr, col, rb;
+        DevBuf<int> ptr, col, rb, wb;
         DevBuf<double> v64;
         DevBuf<float> v32;
     };
