@@ -333,7 +333,8 @@ __global__ void __launch_bounds__(TPB) k_sell_residual(DevSell<T> A, const T* b,
 // row blocks b = blockIdx.x, + gridDim.x, ... through a two-stage ring: the column indices and
 // values of the next row block are copied into shared memory (cp.async.bulk on an mbarrier, 16-byte
 // aligned supersets of the ranges) while the current one gathers x and sums; one thread per row
-// sums its products in order, so the result does not depend on the launch shape. Vectors written
+// sums its products in order (or, for long rows, 8 threads per row in a fixed strided order and
+// shuffle tree), so the result does not depend on the launch shape. Vectors written
 // by earlier kernels of the cycle are read with plain loads after the programmatic-launch wait
 // (never ld.global.nc, which the compiler may move above it); the matrix may be read before it.
 // op: 0 y = M x (restriction); 1 y = omega dinv (b + r) + M x (prolongation with the smoothing
@@ -348,9 +349,12 @@ struct CsrSmem {
     static_assert(col_bytes % 16 == 0 && val_bytes % 16 == 0, "16-byte stage layout");
 };
 
-template <int OP, typename T>
+template <int OP, typename T, int LPR>
 __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega, const T* b, const T* x, T* y,
                                              const T* r) {
+    // LPR threads per row: 1 (each thread sums up to CSR_RPT rows) or 8 for long rows (a row's
+    // products summed by 8 threads, strided, then a fixed shuffle tree; at most TPB / 8 rows)
+    constexpr int RQ = LPR == 1 ? CSR_RPT : 1;
     using L = CsrSmem<T>;
     constexpr int J = CSR_CAP / TPB;
     constexpr int VA = 16 / int(sizeof(T));  // values per 16 bytes
@@ -386,11 +390,11 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
         const int2 a = __ldg(M.rb + blk), z = __ldg(M.rb + blk + 1);
         const int ne = z.y - a.y;
         const bool staged = ne > 0 && ne <= CSR_CAP;
-        int lo[CSR_RPT], hi[CSR_RPT];
-        T ep[CSR_RPT];  // the epilogue's vector operands, loaded before the gathers (independent of them)
+        int lo[RQ], hi[RQ];
+        T ep[RQ];  // the epilogue's vector operands, loaded before the gathers (independent of them)
 #pragma unroll
-        for (int q = 0; q < CSR_RPT; ++q) {
-            const int row = a.x + t + q * TPB;
+        for (int q = 0; q < RQ; ++q) {
+            const int row = LPR == 1 ? a.x + t + q * TPB : a.x + t / LPR;
             lo[q] = hi[q] = 0;
             ep[q] = T(0);
             if (row < z.x) {
@@ -431,9 +435,9 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
             fence_proxy_async_smem();
             issue(blk + 2 * G, s);
         }
-        T acc[CSR_RPT];
+        T acc[RQ];
 #pragma unroll
-        for (int q = 0; q < CSR_RPT; ++q) acc[q] = T(0);
+        for (int q = 0; q < RQ; ++q) acc[q] = T(0);
         if (staged) {
 #pragma unroll
             for (int j = 0; j < J; ++j) {
@@ -441,9 +445,15 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
                 if (k < ne) prod[k] = v[j] * x[c[j]];
             }
             __syncthreads();
+            if (LPR == 1) {
 #pragma unroll
-            for (int q = 0; q < CSR_RPT; ++q)
-                for (int k = lo[q]; k < hi[q]; ++k) acc[q] += prod[k];
+                for (int q = 0; q < RQ; ++q)
+                    for (int k = lo[q]; k < hi[q]; ++k) acc[q] += prod[k];
+            } else {
+                for (int k = lo[0] + t % LPR; k < hi[0]; k += LPR) acc[0] += prod[k];
+#pragma unroll
+                for (int off = LPR / 2; off; off >>= 1) acc[0] += __shfl_down_sync(0xffffffffu, acc[0], off, LPR);
+            }
             __syncthreads();  // prod is rewritten by the next row block
         } else if (ne > CSR_CAP) {  // one long row: strided partial sums, fixed-order block reduction
             T part = T(0);
@@ -460,9 +470,9 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
             __syncthreads();
         }
 #pragma unroll
-        for (int q = 0; q < CSR_RPT; ++q) {
-            const int row = a.x + t + q * TPB;
-            if (row >= z.x) continue;
+        for (int q = 0; q < RQ; ++q) {
+            const int row = LPR == 1 ? a.x + t + q * TPB : a.x + t / LPR;
+            if (row >= z.x || (LPR > 1 && t % LPR != 0)) continue;
             if (OP == 0)
                 y[row] = acc[q];
             else if (OP == 1)
@@ -473,26 +483,28 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
     }
 }
 
-// ---- CSR in warp blocks: a warp takes up to 32 consecutive rows holding at most WS_CAP entries.
-// Lane l loads the block's entries l, l + 32, ... (coalesced) into registers before the
+// ---- CSR in warp blocks: a warp takes up to 32 / LPR consecutive rows holding at most WS_CAP
+// entries. Lane l loads the block's entries l, l + 32, ... (coalesced) into registers before the
 // programmatic-launch wait (the matrix is never written by the cycle), gathers x after it and
-// stores the products in the warp's slice of shared memory; lane i then sums row i's products in
-// order (deterministic). A row longer than WS_CAP is a block of its own, summed by the whole warp
-// from global memory (strided partial sums, fixed shuffle tree). Same ops as k_csr.
+// stores the products in the warp's slice of shared memory; the LPR lanes of a row then sum its
+// products (LPR = 1: in order; LPR = 8 for long rows: strided, then a fixed shuffle tree), so the
+// result is deterministic. A row longer than WS_CAP is a block of its own, summed by the whole
+// warp from global memory (strided partial sums, fixed shuffle tree). Same ops as k_csr.
 constexpr int WS_CAP = 128, WS_J = WS_CAP / 32, WS_WARPS = 8;
-template <int OP, typename T>
+template <int OP, typename T, int LPR>
 __global__ void __launch_bounds__(WS_WARPS * 32) k_csr_ws(DevCsr<T> M, const T* dinv, T omega, const T* b,
                                                           const T* x, T* y, const T* r) {
     __shared__ T prod[WS_WARPS][WS_CAP];
     pdl_trigger();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, blk = blockIdx.x * WS_WARPS + w;
+    const int rl_i = lane / LPR, sub = lane % LPR;  // LPR lanes per row (at most 32 / LPR rows)
     const bool live = blk < M.nwb;
     int2 a = make_int2(0, 0), z = make_int2(0, 0);
     if (live) {
         a = __ldg(M.wb + blk);
         z = __ldg(M.wb + blk + 1);
     }
-    const int ne = z.y - a.y, row = a.x + lane;
+    const int ne = z.y - a.y, row = a.x + rl_i;
     const bool rl = row < z.x;
     const bool staged = ne <= WS_CAP;
     int lo = 0, hi = 0;
@@ -527,13 +539,20 @@ __global__ void __launch_bounds__(WS_WARPS * 32) k_csr_ws(DevCsr<T> M, const T* 
             if (k < ne) prod[w][k] = v[j] * x[c[j]];
         }
         __syncwarp();
-        if (rl)
-            for (int k = lo; k < hi; ++k) acc += prod[w][k];
+        if (LPR == 1) {
+            if (rl)
+                for (int k = lo; k < hi; ++k) acc += prod[w][k];
+        } else {
+            if (rl)
+                for (int k = lo + sub; k < hi; k += LPR) acc += prod[w][k];
+#pragma unroll
+            for (int off = LPR / 2; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off, LPR);
+        }
     } else {
         for (int k = lane; k < ne; k += 32) acc += __ldg(M.val + a.y + k) * x[__ldg(M.col + a.y + k)];
         for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
     }
-    if (rl && (staged || lane == 0)) {
+    if (rl && (staged ? sub == 0 : lane == 0)) {
         if (OP == 0)
             y[row] = acc;
         else if (OP == 1)
@@ -544,12 +563,17 @@ __global__ void __launch_bounds__(WS_WARPS * 32) k_csr_ws(DevCsr<T> M, const T* 
 }
 
 
+template <int OP, typename T, int LPR>
+void prepare_csr_op1() {
+    VG_CUDA(cudaFuncSetAttribute(k_csr<OP, T, LPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, CsrSmem<T>::total));
+    // the whole unified L1/shared array as shared memory: the occupancy the grid is sized for
+    VG_CUDA(cudaFuncSetAttribute(k_csr<OP, T, LPR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 int(cudaSharedmemCarveoutMaxShared)));
+}
 template <int OP, typename T>
 void prepare_csr_op() {
-    VG_CUDA(cudaFuncSetAttribute(k_csr<OP, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, CsrSmem<T>::total));
-    // the whole unified L1/shared array as shared memory: the occupancy the grid is sized for
-    VG_CUDA(cudaFuncSetAttribute(k_csr<OP, T>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 int(cudaSharedmemCarveoutMaxShared)));
+    prepare_csr_op1<OP, T, 1>();
+    prepare_csr_op1<OP, T, 8>();
 }
 
 // kernel attributes on the current device (function attributes are per device) and the number of
@@ -564,8 +588,8 @@ void prepare_csr_kernels(int slots[2]) {
     int dev = 0, n32 = 0, n64 = 0, sms = 0;
     VG_CUDA(cudaGetDevice(&dev));
     VG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n32, k_csr<0, float>, TPB, CsrSmem<float>::total));
-    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n64, k_csr<0, double>, TPB, CsrSmem<double>::total));
+    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n32, k_csr<0, float, 1>, TPB, CsrSmem<float>::total));
+    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n64, k_csr<0, double, 1>, TPB, CsrSmem<double>::total));
     slots[0] = std::max(1, n32) * std::max(1, sms);
     slots[1] = std::max(1, n64) * std::max(1, sms);
 }
@@ -577,9 +601,24 @@ void launch_csr(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, 
     const int grid = std::min(M.nblk, std::max(1, M.slots));
     const int sb = CsrSmem<T>::total;
     switch (op) {
-    case 0: launch_pdl(k_csr<0, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
-    case 1: launch_pdl(k_csr<1, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
-    default: launch_pdl(k_csr<2, T>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r); break;
+    case 0:
+        if (M.lpr > 1)
+            launch_pdl(k_csr<0, T, 8>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r);
+        else
+            launch_pdl(k_csr<0, T, 1>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r);
+        break;
+    case 1:
+        if (M.lpr > 1)
+            launch_pdl(k_csr<1, T, 8>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r);
+        else
+            launch_pdl(k_csr<1, T, 1>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r);
+        break;
+    default:
+        if (M.lpr > 1)
+            launch_pdl(k_csr<2, T, 8>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r);
+        else
+            launch_pdl(k_csr<2, T, 1>, grid, TPB, sb, s, M, dinv, omega, b, x, y, r);
+        break;
     }
 }
 
@@ -589,15 +628,32 @@ void launch_ws(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, c
     if (M.n <= 0 || M.nwb <= 0) return;
     const int grid = (M.nwb + WS_WARPS - 1) / WS_WARPS;
     switch (op) {
-    case 0: launch_pdl(k_csr_ws<0, T>, grid, WS_WARPS * 32, 0, s, M, dinv, omega, b, x, y, r); break;
-    case 1: launch_pdl(k_csr_ws<1, T>, grid, WS_WARPS * 32, 0, s, M, dinv, omega, b, x, y, r); break;
-    default: launch_pdl(k_csr_ws<2, T>, grid, WS_WARPS * 32, 0, s, M, dinv, omega, b, x, y, r); break;
+    case 0:
+        if (M.lpr > 1)
+            launch_pdl(k_csr_ws<0, T, 8>, grid, WS_WARPS * 32, 0, s, M, dinv, omega, b, x, y, r);
+        else
+            launch_pdl(k_csr_ws<0, T, 1>, grid, WS_WARPS * 32, 0, s, M, dinv, omega, b, x, y, r);
+        break;
+    case 1:
+        if (M.lpr > 1)
+            launch_pdl(k_csr_ws<1, T, 8>, grid, WS_WARPS * 32, 0, s, M, dinv, omega, b, x, y, r);
+        else
+            launch_pdl(k_csr_ws<1, T, 1>, grid, WS_WARPS * 32, 0, s, M, dinv, omega, b, x, y, r);
+        break;
+    default:
+        if (M.lpr > 1)
+            launch_pdl(k_csr_ws<2, T, 8>, grid, WS_WARPS * 32, 0, s, M, dinv, omega, b, x, y, r);
+        else
+            launch_pdl(k_csr_ws<2, T, 1>, grid, WS_WARPS * 32, 0, s, M, dinv, omega, b, x, y, r);
+        break;
     }
 }
 
 // the CSR product of the cycle in each precision's faster form (1M cells, A/B of builds): FP64 in
 // warp blocks (FP64 solve 22.3 -> 21.5 ms; the row-block kernel holds 3 CTAs per SM in FP64), FP32
-// in row blocks (warp blocks 14.34 -> 14.46 ms)
+// in row blocks (warp blocks 14.34 -> 14.46 ms). Matrices of 16 or more entries per row (the
+// restrictions, the denser coarse operators) are summed by 8 threads per row in both kernels
+// (mixed 14.31 -> 14.13 ms, FP64 21.49 -> 21.14 ms)
 template <typename T>
 void launch_prod(int op, const DevCsr<T>& M, const T* dinv, T omega, const T* b, const T* x, T* y, const T* r,
                  cudaStream_t s) {
@@ -970,11 +1026,13 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
             // between 256 and CSR_CAP (a longer single row is a block of its own)
             const long long nnz = (long long)M.col.size();
             const int cap = int(std::min<long long>(CSR_CAP, std::max<long long>(256, (nnz + 591) / 592)));
+            S.lpr = avg >= 16.0 ? 8 : 1;
+            const int max_rows = S.lpr == 1 ? CSR_RPT * TPB : TPB / S.lpr;
             S.rb.assign({0, 0});
             for (int r = 0; r < M.n;) {
                 const int start = r;
                 long long nn = 0;
-                while (r < M.n && r - start < CSR_RPT * TPB) {
+                while (r < M.n && r - start < max_rows) {
                     const int len = M.ptr[r + 1] - M.ptr[r];
                     if (r > start && nn + len > cap) break;
                     nn += len;
@@ -987,7 +1045,7 @@ void Amg::setup(const HostCsr& S0, const HostCsr* first_P, const std::vector<int
             for (int r = 0; r < M.n;) {
                 const int start = r;
                 long long nn = 0;
-                while (r < M.n && r - start < 32) {
+                while (r < M.n && r - start < 32 / S.lpr) {
                     const int len = M.ptr[r + 1] - M.ptr[r];
                     if (r > start && nn + len > WS_CAP) break;
                     nn += len;
@@ -1202,6 +1260,7 @@ DevCsr<T> Amg::cview(const Sell& S, const CsrBufs& B) const {
     v.n = S.n;
     v.nblk = S.csr ? int(S.rb.size() / 2) - 1 : 0;
     v.slots = csr_slots_[sizeof(T) == 8 ? 1 : 0];
+    v.lpr = S.lpr;
     v.err = const_cast<int*>(err_.data());
     v.rb = reinterpret_cast<const int2*>(B.rb.data());
     v.nwb = S.csr ? int(S.wb.size() / 2) - 1 : 0;

@@ -45,6 +45,7 @@ template <typename T>
 struct DevCsr {
     int n = 0, nblk = 0;
     int slots = 1;  // CTAs of the kernel resident at once on the device (grid cap)
+    int lpr = 1;    // threads per row in the row-block kernel's sums (1, or 8 for long rows)
     const int2* rb = nullptr;
     int* err = nullptr;  // set to 1 when a staged copy never lands (never in a correct run)
     const int* ptr = nullptr;
@@ -97,6 +98,7 @@ private:
         // CSR copy used instead of the slices when rows are long
         bool csr = false;
         std::vector<int> cptr, ccol;
+        int lpr = 1;          // threads per row of the row-block sums
         std::vector<int> rb;  // row blocks: (first row, first entry) pairs, one past the last block included
         std::vector<int> wb;  // warp blocks (at most 32 rows and WS_CAP entries), same layout
         std::vector<double> cval;
