@@ -314,17 +314,21 @@ __device__ __forceinline__ T sell_finish(const DevSell<T>& M, const SellRow<T>& 
 }
 
 // residual of one Jacobi step from zero, r = b - (A S) b, on the SELL-32 finest level (the stored
-// values are those of A S, so only b is gathered). b is written by an earlier kernel: read with
-// plain loads after the programmatic-launch wait (never ld.global.nc, which the compiler may move
-// above it)
+// values are those of A S, so only b is gathered), written as the prolongation's term
+// q = S (b + r). b is written by an earlier kernel: read with plain loads after the
+// programmatic-launch wait (never ld.global.nc, which the compiler may move above it)
 template <typename T>
-__global__ void __launch_bounds__(TPB) k_sell_residual(DevSell<T> A, const T* b, T* r) {
+__global__ void __launch_bounds__(TPB) k_sell_residual(DevSell<T> A, const T* dinv, T omega, const T* b, T* q) {
     pdl_trigger();
     const int i = blockIdx.x * TPB + threadIdx.x;
     SellRow<T> R;
     if (i < A.n) sell_fetch<T>(A, i, R);
+    const T di = i < A.n ? __ldg(dinv + i) : T(0);
     pdl_wait();
-    if (i < A.n) r[i] = b[i] - sell_finish<T>(A, R, b);
+    if (i < A.n) {
+        const T bi = b[i], ri = bi - sell_finish<T>(A, R, b);
+        q[i] = omega * di * (bi + ri);
+    }
 }
 
 // ---- CSR in row blocks (the CSR-stream scheme of Greathouse and Daga, SC 2014, with the entries
@@ -337,8 +341,9 @@ __global__ void __launch_bounds__(TPB) k_sell_residual(DevSell<T> A, const T* b,
 // shuffle tree), so the result does not depend on the launch shape. Vectors written
 // by earlier kernels of the cycle are read with plain loads after the programmatic-launch wait
 // (never ld.global.nc, which the compiler may move above it); the matrix may be read before it.
-// op: 0 y = M x (restriction); 1 y = omega dinv (b + r) + M x (prolongation with the smoothing
-//     of the composite cycle); 2 y = b - M x (residual, with x = b and M = A S)
+// op: 0 y = M x (restriction); 1 y = r + M x (prolongation, r holding S (b + residual) of the
+//     composite cycle); 2 y = omega dinv (b + (b - M x)) (that smoothed residual term, with x = b
+//     and M = A S)
 template <typename T>
 struct CsrSmem {
     static constexpr int col_bytes = (CSR_CAP + 8) * 4;
@@ -391,19 +396,21 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
         const int ne = z.y - a.y;
         const bool staged = ne > 0 && ne <= CSR_CAP;
         int lo[RQ], hi[RQ];
-        T ep[RQ];  // the epilogue's vector operands, loaded before the gathers (independent of them)
+        T ep[RQ], dd[RQ];  // the epilogue's vector operands, loaded before the gathers (independent of them)
 #pragma unroll
         for (int q = 0; q < RQ; ++q) {
             const int row = LPR == 1 ? a.x + t + q * TPB : a.x + t / LPR;
             lo[q] = hi[q] = 0;
-            ep[q] = T(0);
+            ep[q] = dd[q] = T(0);
             if (row < z.x) {
                 lo[q] = __ldg(M.ptr + row) - a.y;
                 hi[q] = __ldg(M.ptr + row + 1) - a.y;
                 if (OP == 1)
-                    ep[q] = omega * __ldg(dinv + row) * (b[row] + r[row]);
-                else if (OP == 2)
+                    ep[q] = r[row];
+                else if (OP == 2) {
                     ep[q] = b[row];
+                    dd[q] = __ldg(dinv + row);
+                }
             }
         }
         int c[J];
@@ -477,8 +484,10 @@ __global__ void __launch_bounds__(TPB) k_csr(DevCsr<T> M, const T* dinv, T omega
                 y[row] = acc[q];
             else if (OP == 1)
                 y[row] = ep[q] + acc[q];
-            else
-                y[row] = ep[q] - acc[q];
+            else {
+                const T rr = ep[q] - acc[q];
+                y[row] = omega * dd[q] * (ep[q] + rr);
+            }
         }
     }
 }
@@ -521,13 +530,13 @@ __global__ void __launch_bounds__(WS_WARPS * 32) k_csr_ws(DevCsr<T> M, const T* 
         c[j] = in ? __ldg(M.col + a.y + k) : 0;
         v[j] = in ? __ldg(M.val + a.y + k) : T(0);
     }
-    const T dl = (OP == 1 && rl) ? __ldg(dinv + row) : T(0);
+    const T dl = (OP == 2 && rl) ? __ldg(dinv + row) : T(0);
     pdl_wait();
     if (!live) return;
     T ep = T(0);
     if (rl) {
         if (OP == 1)
-            ep = omega * dl * (b[row] + r[row]);
+            ep = r[row];
         else if (OP == 2)
             ep = b[row];
     }
@@ -557,8 +566,10 @@ __global__ void __launch_bounds__(WS_WARPS * 32) k_csr_ws(DevCsr<T> M, const T* 
             y[row] = acc;
         else if (OP == 1)
             y[row] = ep + acc;
-        else
-            y[row] = ep - acc;
+        else {
+            const T rr = ep - acc;
+            y[row] = omega * dl * (ep + rr);
+        }
     }
 }
 
@@ -1276,8 +1287,8 @@ DevCsr<T> Amg::cview(const Sell& S, const CsrBufs& B) const {
 
 // one level of the composite V(1,1) cycle (the same operator as Jacobi pre-smoothing from zero,
 // residual, restriction, coarse correction, prolongation and Jacobi post-smoothing):
-//   side stream:  r = b - (A S) b
-//   this stream:  b_c = Rt b;  x_c = cycle(b_c);  z = S (b + r) + Pt x_c
+//   side stream:  q = S (b + r), r = b - (A S) b   (stored in the level's r buffer)
+//   this stream:  b_c = Rt b;  x_c = cycle(b_c);  z = q + Pt x_c
 template <typename T>
 void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     Level& L = levels_[l];
@@ -1302,9 +1313,9 @@ void Amg::cycle(int l, const T* b, T* z, cudaStream_t s) {
     VG_CUDA(cudaEventRecord(ev_fork_[l], s));
     VG_CUDA(cudaStreamWaitEvent(side_, ev_fork_[l], 0));
     if (L.A.csr)
-        launch_prod<T>(2, cview<T>(L.A, L.cA), nullptr, T(0), b, b, r, nullptr, side_);
+        launch_prod<T>(2, cview<T>(L.A, L.cA), dinv, T(L.omega), b, b, r, nullptr, side_);
     else
-        launch_pdl(k_sell_residual<T>, blocks(L.n), TPB, 0, side_, view<T>(L), b, r);
+        launch_pdl(k_sell_residual<T>, blocks(L.n), TPB, 0, side_, view<T>(L), dinv, T(L.omega), b, r);
     VG_CUDA(cudaEventRecord(ev_join_[l], side_));
     launch_prod<T>(0, cview<T>(L.Rt, L.cRt), nullptr, T(0), nullptr, b, bc, nullptr, s);
     cycle<T>(l + 1, bc, xc, s);
