@@ -1142,9 +1142,14 @@ void Solver::minres_t(const T* r, T* x, double tol, int maxit, int check_every, 
         }
     }
     iters = h_flags[2];
-    // kernels per iteration: apply, update, step (+ V-cycle and finish with multigrid)
-    const long long per = 3 + (use_amg ? 1 + 4LL * (amg_levels - 1) + 1 : 0);
-    n_launch += 2 + (use_amg ? 4LL * (amg_levels - 1) + 2 : 0) + per * iters + (iters + 2) / 2;
+    // kernels per iteration: apply, update (flux and pressure rows apart with multigrid), step, and
+    // with multigrid the composite V-cycle (residual, restriction and prolongation per level, the
+    // dense coarsest product) and the finish
+    const long long plo_hi = use_amg ? nf + np : 0;
+    const long long vc = use_amg ? 3LL * (amg_levels - 1) + 1 : 0;
+    const long long upd = (use_amg && plo_hi == N) ? 2 : 1;
+    const long long per = 2 + upd + (use_amg ? vc + 1 : 0);
+    n_launch += 2 + (use_amg ? vc + 1 : 0) + per * iters + (iters + 2) / 2;
     n_apply += iters;
     n_iter += iters;
 }
