@@ -241,6 +241,11 @@ int vg_ms_step(vg_handle* h, const double* old_state, double* new_state, const v
  * VG_ENOCONV otherwise. vg_ms_picard_info reports the last step's iterations, change and residual. */
 int vg_ms_set_picard(vg_handle* h, int max_iterations, double tol);
 int vg_ms_picard_info(const vg_handle* h, int* iterations, double* change, double* nonlinear_residual);
+/* Gram-Schmidt work of the Maxwell-Stefan GMRES since the handle was created: Arnoldi steps and
+ * how many of them ran the second classical Gram-Schmidt pass. The second pass runs only when the
+ * first removed more than half of |w|^2 (selective reorthogonalisation, Daniel-Gragg-Kaufman-
+ * Stewart). No counterpart in the reference (its Krylov solves are PETSc's). */
+int vg_ms_gs_info(const vg_handle* h, long long* arnoldi_steps, long long* reorthogonalizations);
 
 /* ---- post-processing ---------------------------------------------------------------------- */
 

@@ -92,10 +92,16 @@ def test_step_matches_direct_solve(case):
     b[2 * o.nf:] = np.r_[areas * x1, areas * x2] / DT
     ref = spla.spsolve(K.tocsc(), b)
     for mode, rtol in (("fp64", 1e-9), ("mixed", 1e-9)):
+        gs0 = ms.gram_schmidt_info()
         new, info = ms.step(s, mode=mode, tol=1e-11)
         assert info["residual"] <= 1e-11
         got = new.cpu().numpy()
         assert np.linalg.norm(got - ref) <= rtol * np.linalg.norm(ref), mode
+        # every Arnoldi step is counted; the second Gram-Schmidt pass runs in at most all of them
+        gs1 = ms.gram_schmidt_info()
+        steps = gs1["arnoldi_steps"] - gs0["arnoldi_steps"]
+        reo = gs1["reorthogonalizations"] - gs0["reorthogonalizations"]
+        assert steps == info["iterations"] and 0 <= reo <= steps, (mode, steps, reo)
 
 
 def test_steps_conserve_mass_and_sum(case):

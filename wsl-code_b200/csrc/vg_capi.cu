@@ -362,6 +362,13 @@ int vg_ms_picard_info(const vg_handle* h, int* iterations, double* change, doubl
     return VG_OK;
 }
 
+int vg_ms_gs_info(const vg_handle* h, long long* arnoldi_steps, long long* reorthogonalizations) {
+    if (!h || !h->s) return VG_EINVAL;
+    if (arnoldi_steps) *arnoldi_steps = h->s->ms_arnoldi_steps_;
+    if (reorthogonalizations) *reorthogonalizations = h->s->ms_reorth_passes_;
+    return VG_OK;
+}
+
 int vg_local(vg_handle* h, int cell, int which, double* out, int* count) {
     return guarded(h, [&](vg::Solver& s) {
         int c = s.local(cell, which, out);

@@ -258,8 +258,19 @@ struct MsKrylov {
     double cs[MS_MAXM], sn[MS_MAXM], g[MS_MAXM + 1], y[MS_MAXM];
     double hd[3 * MS_MAXM];  // [0, 32): first Gram-Schmidt pass, [32, 64): second, [64]: |w|^2, [65]: |t|^2
     double beta0, tol, rel;
-    int j, its, m, maxit, done, pad_;
+    int j, its, m, maxit, done, reorth;  // reorth: second Gram-Schmidt passes run in this solve
 };
+
+// Selective reorthogonalisation (Daniel, Gragg, Kaufman and Stewart, Math. Comp. 30 (1976); the
+// "twice is enough" analysis of Giraud, Langou and Rozloznik, Comput. Math. Appl. 50 (2005)): the
+// second classical Gram-Schmidt pass runs only when the first removed more than half of |w|^2,
+// i.e. when |w'|^2 < REORTH_ETA2 |w|^2; otherwise w' is already orthogonal to the basis to working
+// precision and the second pass would subtract nothing. hd[cnt] holds |w|^2 before the first pass
+// (written by that pass's dot products), hd[2 MS_MAXM] |w'|^2 after it.
+constexpr double REORTH_ETA2 = 0.5;
+__device__ __forceinline__ bool reorth_skip(const double* hd, int cnt) {
+    return hd[2 * MS_MAXM] >= REORTH_ETA2 * hd[cnt];
+}
 
 // one V-cycle-sized work split: block b owns rows [b chunk, (b + 1) chunk); chunk is a multiple of 4
 template <typename T>
@@ -295,15 +306,24 @@ __device__ void ms_grid_sum(double (*sh)[MS_MAXM], int cnt, double* partials, un
 
 // out[k] = V[:, k] . w for k < cnt, cnt = (cnt_dev ? *cnt_dev : 0) + cnt_add. Block b stages its
 // rows of w in shared memory and streams the cnt columns over them (four at a time, 16-byte
-// loads); the column stride ld and chunk are multiples of 4.
+// loads); the column stride ld and chunk are multiples of 4. self_dot: also out[cnt] = w . w (the
+// first Gram-Schmidt pass, for the reorthogonalisation test). reo: the second pass; when
+// reorth_skip(reo, cnt) holds, out[0..cnt) = 0 and nothing is read.
 template <typename T>
 __global__ void __launch_bounds__(MS_THREADS) k_mdot(const T* V, long long ld, const int* cnt_dev, int cnt_add,
                                                      const T* w, long long n, long long chunk, double* partials,
-                                                     unsigned* counter, double* out) {
+                                                     unsigned* counter, double* out, int self_dot,
+                                                     const double* reo) {
     extern __shared__ __align__(16) unsigned char ms_smem[];
     T* ws = reinterpret_cast<T*>(ms_smem);
     __shared__ double sh[MS_THREADS / 32][MS_MAXM];
     const int cnt = min((cnt_dev ? *cnt_dev : 0) + cnt_add, MS_MAXM);
+    if (reo && reorth_skip(reo, cnt)) {
+        if (blockIdx.x == 0 && threadIdx.x < cnt) out[threadIdx.x] = 0.0;
+        return;
+    }
+    const bool sd = self_dot && cnt < MS_MAXM;
+    double aw = 0;
     const long long lo = blockIdx.x * chunk;
     const int len = int(max(0LL, min(n, lo + chunk) - lo));
     const int len4 = len & ~3;
@@ -335,6 +355,7 @@ __global__ void __launch_bounds__(MS_THREADS) k_mdot(const T* V, long long ld, c
             a1 += dot4(p1, x);
             a2 += dot4(p2, x);
             a3 += dot4(p3, x);
+            if (sd && k == 0) aw += dot4(x, x);
         }
         for (int i = len4 + threadIdx.x; i < len; i += MS_THREADS) {
             const double xi = double(ws[i]);
@@ -342,6 +363,7 @@ __global__ void __launch_bounds__(MS_THREADS) k_mdot(const T* V, long long ld, c
             a1 += double(v1[i]) * xi;
             a2 += double(v2[i]) * xi;
             a3 += double(v3[i]) * xi;
+            if (sd && k == 0) aw += xi * xi;
         }
         for (int off = 16; off; off >>= 1) {
             a0 += __shfl_down_sync(0xffffffffu, a0, off);
@@ -356,18 +378,30 @@ __global__ void __launch_bounds__(MS_THREADS) k_mdot(const T* V, long long ld, c
             if (nk > 3) sh[wid][k + 3] = a3;
         }
     }
+    if (sd) {
+        for (int off = 16; off; off >>= 1) aw += __shfl_down_sync(0xffffffffu, aw, off);
+        if (l == 0) sh[wid][cnt] = aw;
+    }
     __syncthreads();
-    ms_grid_sum(sh, cnt, partials, counter, out);
+    ms_grid_sum(sh, cnt + (sd ? 1 : 0), partials, counter, out);
 }
 
-// w -= sum_k h[k] V[:, k] (cnt columns, as in k_mdot); with nrm: |w|^2 of the result -> nrm[0]
+// w -= sum_k h[k] V[:, k] (cnt columns, as in k_mdot); with nrm: |w|^2 of the result -> nrm[0].
+// reo: the second pass; skipped when reorth_skip(reo, cnt) holds (w and nrm keep the first pass's
+// values), otherwise counted in *runs.
 template <typename T>
 __global__ void __launch_bounds__(MS_THREADS) k_gs_update(const T* V, long long ld, const int* cnt_dev, int cnt_add,
                                                           const double* h, T* w, long long n, double* partials,
-                                                          unsigned* counter, double* nrm) {
+                                                          unsigned* counter, double* nrm, const double* reo,
+                                                          int* runs) {
     __shared__ T hs[MS_MAXM];
     __shared__ double sh[MS_THREADS / 32][MS_MAXM];
     const int cnt = min((cnt_dev ? *cnt_dev : 0) + cnt_add, MS_MAXM);
+    if (reo) {
+        // every block reads nrm[0] here, before any block can reach the grid sum that rewrites it
+        if (reorth_skip(reo, cnt)) return;
+        if (runs && blockIdx.x == 0 && threadIdx.x == 0) *runs += 1;
+    }
     if (threadIdx.x < cnt) hs[threadIdx.x] = T(h[threadIdx.x]);
     __syncthreads();
     const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nth = (long long)gridDim.x * blockDim.x;
@@ -455,6 +489,7 @@ __global__ void k_kry_init(MsKrylov* K, double tol, int m, int maxit) {
     K->its = 0;
     K->done = 0;
     K->rel = 1.0;
+    K->reorth = 0;
 }
 
 // end of an Arnoldi step: Hessenberg column j from the two Gram-Schmidt passes, previous rotations,
@@ -722,7 +757,7 @@ void Solver::ms_build_amg() {
 template <typename T>
 void Solver::ms_norm2(const T* x, double* dst) {
     k_mdot<T><<<ms_.dblocks, MS_THREADS, ms_.chunk * sizeof(T), stream_>>>(
-        x, 0, nullptr, 1, x, ms_.N, ms_.chunk, ms_.partials.data(), ms_.counter.data(), dst);
+        x, 0, nullptr, 1, x, ms_.N, ms_.chunk, ms_.partials.data(), ms_.counter.data(), dst, 0, nullptr);
     VG_CUDA(cudaGetLastError());
 }
 
@@ -762,11 +797,14 @@ void Solver::ms_arnoldi_step(cudaGraphConditionalHandle cond) {
     const size_t smem = ms_.chunk * sizeof(T);
     ms_precond<T>(vn, t);
     ms_apply<T>(t, w);
+    // first pass (with |w|^2 for the test), then the second only where the test asks for it
     for (int pass = 0; pass < 2; ++pass) {
         double* hd = K->hd + pass * MS_MAXM;
-        k_mdot<T><<<ms_.dblocks, MS_THREADS, smem, stream_>>>(V, ld, &K->j, 1, w, Nm, ms_.chunk, part, ctr, hd);
+        const double* reo = pass ? K->hd : nullptr;
+        k_mdot<T><<<ms_.dblocks, MS_THREADS, smem, stream_>>>(V, ld, &K->j, 1, w, Nm, ms_.chunk, part, ctr, hd,
+                                                              pass ? 0 : 1, reo);
         k_gs_update<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(V, ld, &K->j, 1, hd, w, Nm, part, ctr,
-                                                              pass ? K->hd + 2 * MS_MAXM : nullptr);
+                                                              K->hd + 2 * MS_MAXM, reo, &K->reorth);
     }
     k_scale_norm<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(w, K->hd + 2 * MS_MAXM, V, ld, &K->j, vn, Nm);
     k_givens<<<1, 1, 0, stream_>>>(K, cond);
@@ -832,7 +870,7 @@ int Solver::ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* 
     if (!ms_.gexec[p]) ms_build_graph<T>(p);
     struct {
         double rel;
-        int its, done;
+        int its, done, reorth;
     } out{};
     for (int first = 1;; first = 0) {
         k_cycle_start<T><<<MS_BLOCKS, MS_THREADS, 0, stream_>>>(t, V, vn, Nm, K, first);
@@ -845,6 +883,7 @@ int Solver::ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* 
         VG_CUDA(cudaMemcpyAsync(&out.rel, &K->rel, sizeof(double), cudaMemcpyDeviceToHost, stream_));
         VG_CUDA(cudaMemcpyAsync(&out.its, &K->its, sizeof(int), cudaMemcpyDeviceToHost, stream_));
         VG_CUDA(cudaMemcpyAsync(&out.done, &K->done, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        VG_CUDA(cudaMemcpyAsync(&out.reorth, &K->reorth, sizeof(int), cudaMemcpyDeviceToHost, stream_));
         VG_CUDA(cudaStreamSynchronize(stream_));
         *rel = out.rel;
         if (out.done || out.its >= maxit) break;
@@ -865,6 +904,8 @@ int Solver::ms_gmres(const T* r, T* d, double tol, int maxit, int mres, double* 
         *rel = beta / beta0;
         if (*rel <= tol || !(beta > 0)) break;
     }
+    ms_arnoldi_steps_ += out.its;
+    ms_reorth_passes_ += out.reorth;
     return out.its;
 }
 

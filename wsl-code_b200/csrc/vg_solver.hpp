@@ -70,6 +70,7 @@ public:
     void ms_set_picard(int max_iterations, double tol);
     int ms_last_picard_ = 0;
     double ms_last_change_ = 0, ms_last_nonlinear_ = 0;
+    long long ms_arnoldi_steps_ = 0, ms_reorth_passes_ = 0;  // GMRES Arnoldi steps, second Gram-Schmidt passes
     int device() const { return device_; }  // the CUDA device that holds this handle's data
     // failure-path test hook and the asynchronous error report of vg_apply
     void inject_apply_stall();

@@ -88,6 +88,7 @@ def lib():
         L.vg_debug_stall_apply.argtypes = [P]
         L.vg_ms_set_picard.argtypes = [P, I, D]
         L.vg_ms_picard_info.argtypes = [P, ctypes.POINTER(I), ctypes.POINTER(D), ctypes.POINTER(D)]
+        L.vg_ms_gs_info.argtypes = [P, ctypes.POINTER(LL), ctypes.POINTER(LL)]
         _lib = L
     return _lib
 

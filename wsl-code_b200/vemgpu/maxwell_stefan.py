@@ -80,5 +80,12 @@ class MaxwellStefan:
         return out, dict(iterations=info.iterations, outer=info.outer, residual=info.residual, seconds=info.seconds,
                          picard=pic.value, picard_change=change.value, nonlinear_residual=nonlin.value)
 
+    def gram_schmidt_info(self):
+        """Arnoldi steps of the handle's GMRES solves so far and how many ran the second
+        Gram-Schmidt pass (selective reorthogonalisation)."""
+        steps, reo = ctypes.c_longlong(), ctypes.c_longlong()
+        L.check(L.lib().vg_ms_gs_info(self.gpu.h, ctypes.byref(steps), ctypes.byref(reo)), self.gpu.h)
+        return dict(arnoldi_steps=steps.value, reorthogonalizations=reo.value)
+
     def close(self):
         self.gpu.close()
