@@ -32,6 +32,7 @@ INNER_TOL = 1e-6  # FP32 inner MINRES: relative reduction per refinement step
 PARITY_TOL = 1e-12  # residual of the solves compared with the oracle
 FD_TOL = 1e-14  # residual of the FP64 forward solves of the finite-difference checks (the FP64 floor)
 GRAD_TOL = 1e-12  # residual of the FP64 adjoint solve of the gradient checks
+CORR_TOL = 1e-12  # residual, relative to its right-hand side, of the FP64 correction solves of the FD check
 
 
 def parse():
@@ -352,7 +353,9 @@ def adjoint_leg(args, rank, job=None):
       contraction; `job`);
     * FP64 central differences (step 1e-6) of J along 20 seeded unit directions, each J from a
       solve to FD_TOL started from the base solution, against the adjoint's directional derivatives,
-      relative to the largest directional derivative."""
+      relative to the largest directional derivative; and the same central differences with the
+      numerator formed from the pressure corrections x(theta +- step v) - x0 (solved for directly),
+      which removes the cancellation between the two values of J."""
     import numpy as np
     import torch
     import vemgpu
@@ -406,10 +409,45 @@ def adjoint_leg(args, rank, job=None):
                                "J_rel_diff": abs(J - r["J"]) / abs(r["J"]), "oracle_seconds": r["seconds"],
                                "oracle": "sparse LU of the 1M-unknown system, adjoint by the transposed factors"}
         job.close()
+
+    # Cancellation-free central differences. K(theta) = [M(theta), -W^T; W, 0] with the flux block
+    # M(theta) = sum_E exp(-theta_E) M_E, so for theta' = theta + sigma step v
+    #   K(theta') x0 = K(theta) x0 + [sum_E s_E exp(-theta_E) M_E u0; 0],  s_E = expm1(-sigma step v_E),
+    # u0 the flux part of x0. The perturbation term is formed by one apply of u0 with the log
+    # permeability theta - log(s + m) (m a power of two above 2 max|s|: a benign uniform shift of the
+    # field) less m times the apply of u0 at theta (exact scaling): its rounding error is relative to
+    # m |s| M u0, not to K x0. The correction e = x(theta') - x0 solves
+    # K(theta') e = (b - K(theta) x0) - perturbation, an FP64 solve to CORR_TOL relative to its own
+    # right-hand side, and J(+) - J(-) = sum_o (p+ - p-)(p+ + p- - 2 d_o) is formed from the two
+    # corrections' observed pressures.
+    b0 = h.rhs()
+    rb0 = b0 - h.apply(x0)
+    base_res = float(torch.linalg.norm(rb0) / torch.linalg.norm(b0))  # sign check of b - K x0
+    u0 = x0.clone()
+    u0[h.nf:] = 0
+    y0 = h.apply(u0)
+    nf = h.nf
+
+    def correction(v, sigma):
+        s = torch.expm1(-sigma * 1e-6 * v)
+        m = 2.0 ** np.ceil(np.log2(2 * float(s.abs().max())))
+        h.set_log_permeability(base - torch.log(s + m))
+        ya = h.apply(u0)
+        r = rb0.clone()
+        r[:nf] -= ya[:nf] - m * y0[:nf]
+        h.set_log_permeability(base + sigma * 1e-6 * v)
+        e = h.zeros()
+        try:
+            h.solve(b=r, x=e, mode="fp64", tol=CORR_TOL)
+        except vemgpu.VemGpuError:
+            pass  # the FP64 floor was reached before CORR_TOL: e is the last iterate
+        return obs.pressure(e)
+
     rng = np.random.default_rng(args.seed + 14)
-    ad, fd = [], []
+    ad, fd, fdc = [], [], []
     t0 = time.time()
     base = torch.tensor(th, dtype=torch.float64, device="cuda")
+    r0 = obs.pressure(x0) - obs.data
     for _ in range(args.fd_directions):
         v = torch.tensor(rng.standard_normal(h.nc), device="cuda")
         v = v / torch.linalg.norm(v)
@@ -417,10 +455,13 @@ def adjoint_leg(args, rank, job=None):
         jp = float(obs(solve_tight(x0)[0]))
         h.set_log_permeability(base - 1e-6 * v)
         jm = float(obs(solve_tight(x0)[0]))
+        dp = correction(v, 1.0)
+        dm = correction(v, -1.0)
         ad.append(float(grad @ v))
         fd.append((jp - jm) / 2e-6)
+        fdc.append(float(((dp - dm) * (2 * r0 + dp + dm)).sum()) / 2e-6)
     h.set_log_permeability(base)
-    ad, fd = np.array(ad), np.array(fd)
+    ad, fd, fdc = np.array(ad), np.array(fd), np.array(fdc)
     # rounding floor of a central difference of J: one unit in the last place of J in each of the
     # two values, divided by 2 step; relative to the largest directional derivative
     ulp = float(np.spacing(abs(J)))
@@ -430,7 +471,14 @@ def adjoint_leg(args, rank, job=None):
                        "max_abs_diff_over_max_abs_derivative": err,
                        "max_abs_diff_over_grad_norm": float(np.abs(ad - fd).max() / gn),
                        "rounding_floor_over_max_abs_derivative": floor, "error_in_floor_units": err / floor,
-                       "max_abs_derivative": float(np.abs(ad).max()), "seconds": time.time() - t0}
+                       "max_abs_derivative": float(np.abs(ad).max()), "seconds": time.time() - t0,
+                       "difference_form": {
+                           "max_abs_diff_over_max_abs_derivative": float(np.abs(ad - fdc).max() / np.abs(ad).max()),
+                           "correction_tol": CORR_TOL, "base_residual_b_minus_Kx0": base_res,
+                           "how": "numerator J(+) - J(-) = sum_o (p+ - p-)(p+ + p- - 2 d_o) from the pressure "
+                                  "corrections e = x(theta +- step v) - x0, each an FP64 solve of "
+                                  "K(theta +- step v) e = b - K(theta) x0 - (K(theta +- step v) - K(theta)) x0, "
+                                  "the last term formed from the per-cell scaling of the flux block"}}
     h.close()
     return out
 
@@ -472,6 +520,7 @@ def ms_leg(args):
     finals = {}
     for mode in ("fp64", "mixed"):
         s = s0.clone()
+        gs0 = ms.gram_schmidt_info()
         its, secs, pics, sum_err, mass_err, lo, hi = [], [], [], 0.0, 0.0, 1.0, 0.0
         for _ in range(args.ms_steps):
             s, info = ms.step(s, mode=mode, tol=1e-10, inner_tol=1e-5)
@@ -484,11 +533,13 @@ def ms_leg(args):
             hi = max(hi, max(float(x.max()) for x in f))
             mass_err = max(mass_err, max(abs(a - b) / abs(b) for a, b in zip(ms.masses(s), m0)))
         finals[mode] = torch.cat(ms.fractions(s)[:2])
+        gs1 = ms.gram_schmidt_info()
         out[mode] = {"total_s": float(np.sum(secs)), "step_ms_mean": 1e3 * float(np.mean(secs)),
                      "iterations_mean": float(np.mean(its)), "iterations_max": int(np.max(its)),
                      "picard_mean": float(np.mean(pics)), "picard_max": int(np.max(pics)),
                      "max_sum_to_one_error": sum_err, "max_rel_mass_change": mass_err, "min_fraction": lo,
-                     "max_fraction": hi}
+                     "max_fraction": hi, "arnoldi_steps": gs1["arnoldi_steps"] - gs0["arnoldi_steps"],
+                     "second_gram_schmidt_passes": gs1["reorthogonalizations"] - gs0["reorthogonalizations"]}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["total_s"] / out["mixed"]["total_s"]
     out["final_rel_diff_mixed_vs_fp64"] = float(torch.linalg.norm(finals["mixed"] - finals["fp64"]) /
                                                 torch.linalg.norm(finals["fp64"]))
@@ -891,6 +942,7 @@ def summary(line):
         out.update(grad_over_solve=r(get(a, "mixed", "grad_over_solve")),
                    grad_vs_cpu=r(get(a, "cpu_gradient", "max_abs_diff_over_max_abs")),
                    fd_vs_max_derivative=r(get(a, "fd_check", "max_abs_diff_over_max_abs_derivative")),
+                   fd_difference_form=r(get(a, "fd_check", "difference_form", "max_abs_diff_over_max_abs_derivative")),
                    fd_floor=r(get(a, "fd_check", "rounding_floor_over_max_abs_derivative")))
     c2 = line.get("disk_250k")
     if c2:
