@@ -48,7 +48,21 @@ namespace {
 #ifndef VG_CTAS_PER_SM
 #define VG_CTAS_PER_SM 2  // FP64; FP32 (fewer registers per cell) runs one more CTA per SM
 #endif
+#ifndef VG_BULK_DIRECT_SPEC
+#define VG_BULK_DIRECT_SPEC 1  // 0: the streamed kernel's direct (oversized) pieces use the generic body
+#endif
+#ifndef VG_BULK_GROUPS
+#define VG_BULK_GROUPS 2
+#endif
 constexpr int BULK_CONSUMERS = VG_BULK_CONSUMERS;       // consumer warps per CTA
+// The consumer warps form BULK_GROUPS groups; group g consumes the stages of batches i with
+// i % BULK_GROUPS == g. A stage holds only 3-4 piece records at k = 0, so a group of a few warps
+// is enough for it, and each warp waits on, walks and releases only its group's stages instead of
+// every stage. The stage count is a multiple of BULK_GROUPS, so a ring slot is always consumed by
+// the same group and every waiter is at most one phase ahead of its slot's barrier.
+constexpr int BULK_GROUPS = VG_BULK_GROUPS;
+constexpr int GROUP_WARPS = BULK_CONSUMERS / BULK_GROUPS;
+static_assert(BULK_CONSUMERS % BULK_GROUPS == 0, "consumer warps split evenly into groups");
 // smallest shared-memory stage and resident CTAs per SM (k = 0), by element size: measured at 1M
 // cells, FP32 runs 3 CTAs of 72 registers per thread with 16 KB stages (apply 39.0 -> 38.0 us),
 // FP64 stays at 2 CTAs of 96 registers (3 CTAs spill and take 70 us instead of 56)
@@ -332,14 +346,16 @@ __host__ __device__ constexpr bool prefetch_all() {
     return N * (N + 1) / 2 <= 48;
 }
 
-// one lane of a piece read from the strided global arrays
-template <typename T, int K>
+// one lane of a piece read from the strided global arrays. SPEC: the cell bodies specialised by
+// edge count; without it every piece takes the generic body (the streamed kernel's rare pieces too
+// large for a stage, where a second set of specialised bodies would only add code)
+template <typename T, int K, bool SPEC = true>
 __device__ __forceinline__ void piece_global(const ApplyArgs<T>& a, const Piece& P, int lane, double& quad,
                                              double& msum) {
     if (lane >= P.count) return;
     GlobalSrc<T> src{a.A + P.a_off + lane, a.W + P.w_off + lane, a.map + P.map_off + lane};
     const int prow = __ldg(a.prow + P.slot + lane);  // first pressure row of the cell
-    if constexpr (K == 0 || K == 1) {
+    if constexpr (SPEC && (K == 0 || K == 1)) {
         switch (P.ne) {
         case 3: cell_apply<T, K, 3, prefetch_all<K, 3>()>(a, src, prow, quad, msum); return;
         case 4: cell_apply<T, K, 4, prefetch_all<K, 4>()>(a, src, prow, quad, msum); return;
@@ -402,7 +418,7 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], BULK_CONSUMERS);
+            mbar_init(&empty[s], GROUP_WARPS);
         }
         mbar_init(&never, 1);
         abort_flag = 0;
@@ -437,16 +453,16 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
             }
         }
     } else {  // consumers
-        const int cw = warp - 1;
+        const int cw = warp - 1, grp = cw / GROUP_WARPS, gw = cw % GROUP_WARPS;
         // test hook (failure-path tests only): the first consumer warp 0 to find the flag set
-        // clears it and, at its CTA's last batch, waits on a barrier nothing arrives on, so that
-        // its bounded wait runs out; the flag is loaded while the first stage is still in flight
+        // clears it and, at the last batch of its group, waits on a barrier nothing arrives on, so
+        // that its bounded wait runs out; the flag is loaded while the first stage is still in flight
         int stall_req = 0;
         if (cw == 0 && lane == 0 && a.stall) stall_req = *reinterpret_cast<volatile int*>(a.stall);
-        for (int i = 0; i < nb; ++i) {
+        for (int i = grp; i < nb; i += BULK_GROUPS) {
             const int s = i % S;
             bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], unsigned(i / S) & 1u, &abort_flag));
-            if (cw == 0 && i == nb - 1) {
+            if (cw == 0 && i + BULK_GROUPS >= nb) {
                 int st = 0;
                 if (lane == 0 && stall_req) st = atomicExch(a.stall, 0);
                 if (__shfl_sync(0xffffffffu, st, 0)) ok = __all_sync(0xffffffffu, mbar_wait(&never, 0u, &abort_flag));
@@ -460,13 +476,13 @@ __global__ void __launch_bounds__(BULK_THREADS, K == 0 ? ctas_per_sm(int(sizeof(
             }
             const int first = st_first[s], count = st_count[s];
             if (st_direct[s]) {
-                for (int j = cw; j < count; j += BULK_CONSUMERS)
-                    piece_global<T, K>(a, a.pieces[first + j], lane, quad, msum);
+                for (int j = gw; j < count; j += GROUP_WARPS)
+                    piece_global<T, K, VG_BULK_DIRECT_SPEC != 0>(a, a.pieces[first + j], lane, quad, msum);
             } else {
                 const unsigned char* r = ring + size_t(s) * SB;
                 for (int j = 0; j < count; ++j) {
                     const int4 h = *reinterpret_cast<const int4*>(r);
-                    if ((first + j) % BULK_CONSUMERS == cw) piece_record<T, K>(a, r, h, lane, quad, msum);
+                    if ((first + j) % GROUP_WARPS == gw) piece_record<T, K>(a, r, h, lane, quad, msum);
                     r += h.w;
                 }
             }
@@ -526,6 +542,8 @@ StreamPlan plan_stream(const std::vector<Piece>& pieces, int k, int elem_bytes, 
     sb = std::min<long long>(sb, 96 << 10);
     pl.stage_bytes = int(sb);
     pl.stages = int(std::max<long long>(2, std::min<long long>(MAX_STAGES, MAX_RING_BYTES / sb)));
+    pl.stages -= pl.stages % BULK_GROUPS;  // a ring slot always belongs to one consumer group
+    static_assert(2 % BULK_GROUPS == 0 && MAX_STAGES % BULK_GROUPS == 0, "at least one stage per group");
     const int per_sm = int(std::max<long long>(
         1, std::min<long long>(k == 0 ? ctas_per_sm(elem_bytes) : 1, (227 << 10) / (pl.stages * sb + 8192))));
     // batches: runs of whole records up to one stage
@@ -601,6 +619,7 @@ template <typename T>
 void launch_apply(ApplyArgs<T> a, cudaStream_t s) {
     if (a.rec && a.k <= 1) {
         if (a.ncta == 0) return;
+        if (a.stages < BULK_GROUPS || a.stages % BULK_GROUPS) throw Error(VG_EINVAL, "apply ring: stage count not a multiple of the consumer groups");
         const size_t smem = size_t(a.stages) * a.stage_bytes;
         if (a.k == 0)
             apply_bulk_kernel<T, 0><<<a.ncta, BULK_THREADS, smem, s>>>(a);
