@@ -49,7 +49,7 @@ namespace {
 #define VG_CTAS_PER_SM 2  // FP64; FP32 (fewer registers per cell) runs one more CTA per SM
 #endif
 #ifndef VG_BULK_DIRECT_SPEC
-#define VG_BULK_DIRECT_SPEC 1  // 0: the streamed kernel's direct (oversized) pieces use the generic body
+#define VG_BULK_DIRECT_SPEC 0  // 1: the streamed kernel's direct (oversized) pieces use the specialised bodies too
 #endif
 #ifndef VG_BULK_GROUPS
 #define VG_BULK_GROUPS 2
