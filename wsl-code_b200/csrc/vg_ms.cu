@@ -9,10 +9,11 @@
 // divergence (W = 1 per local edge moment at k = 0). The reference treats all three species with a
 // regularised coupling and Picard iterations (vem/CurvedVEM_Darcy_gpu/src/equation_gpu.cu:111-146,
 // include/problem_device.cuh:12-28, src/solver_driver.cpp:202-240); here the third species is
-// eliminated and B is frozen at x^n (one linear solve per step).
+// eliminated; B is taken at x^n (one linear solve per step, the default) or, with Picard
+// iterations (vg_ms_set_picard), re-evaluated at the latest iterate until the step is fully implicit.
 //
 // B is not symmetric, so the system is solved by right-preconditioned GMRES(m) (classical
-// Gram-Schmidt applied twice; the Arnoldi loop of a cycle is a captured CUDA graph whose Hessenberg
+// Gram-Schmidt, a second pass where the first lost too much of |w|; the Arnoldi loop of a cycle is a captured CUDA graph whose Hessenberg
 // column, Givens rotations and residual estimate are formed on the device), FP64 or
 // FP32 inner under FP64 iterative refinement, with a block-diagonal preconditioner: the 2x2 species
 // block of the assembled flux diagonal per flux dof, and for each species one smoothed-aggregation
@@ -782,7 +783,8 @@ void Solver::ms_destroy_graphs() {
 }
 
 // one Arnoldi step on the stream being captured: z = M^{-1} v_j, w = K z, classical Gram-Schmidt
-// applied twice (the second pass restores the orthogonality lost to cancellation), v_{j+1} = w/|w|,
+// with a second pass where the first removed more than half of |w|^2 (it restores the
+// orthogonality lost to cancellation), v_{j+1} = w/|w|,
 // then the Givens update that sets the loop condition. The column index j lives on the device.
 template <typename T>
 void Solver::ms_arnoldi_step(cudaGraphConditionalHandle cond) {
