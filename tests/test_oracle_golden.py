@@ -141,3 +141,50 @@ def test_reference_cpu_solver_matches_direct_solve(k):
     assert it > 0 and tm["rel"] <= 1e-10
     assert np.linalg.norm(b - K @ x) <= 1e-8 * np.linalg.norm(b)
     assert np.linalg.norm(x - xo) <= 1e-7 * np.linalg.norm(xo)
+
+
+def test_permeability_perturbation_identity():
+    """The identity behind the cancellation-free finite differences of the adjoint checks. The flux
+    block scales per cell with exp(-theta_E) and the divergence block does not depend on theta, so
+    K(theta + h v) x - K(theta) x = [sum_E s_E A_E(theta) u_E; 0] with s_E = expm1(-h v_E) and u the
+    flux part of x; that term equals the flux rows of K(theta - log(s + m)) u - m K(theta) u for a
+    power of two m above 2 max|s|, and computed so it is accurate to its own size, while the plain
+    difference of the two products is accurate only to the rounding of K x (about 1e-16 / h)."""
+    from vemgpu import meshgen
+    m = meshgen.voronoi_mesh(300, "annulus", seed=5)
+    nc = len(m["cell_ptr"]) - 1
+    rng = np.random.default_rng(6)
+    th = rng.normal(0.0, 1.0, nc)
+    v = rng.standard_normal(nc)
+    v /= np.linalg.norm(v)
+    h = 1e-6
+    s = np.expm1(-h * v)
+    mm = 2.0 ** np.ceil(np.log2(2 * np.abs(s).max()))
+
+    def oracle(theta):
+        return O.Oracle(m, k=0, geom=O.GEOM_ARCS, problem=O.PROB_ANNULUS, bc=O.BC_PRESSURE, theta=theta)
+    o0 = oracle(th)
+    K0 = o0.system()[0]
+    Kp = oracle(th + h * v).system()[0]
+    Ka = oracle(th - np.log(s + mm)).system()[0]
+    nf = o0.nf
+    x = rng.standard_normal(o0.N)
+    u = x.copy()
+    u[nf:] = 0
+    # per-cell reference: sum_E s_E A_E(theta) u_E with the oracle's own dof map and directions
+    ref = np.zeros(o0.N)
+    for c in range(nc):
+        d = o0.local(c, "dir")
+        n = len(d)
+        gd = o0.local(c, "gdofs")[:n].astype(np.int64)
+        A = o0.local(c, "A").reshape(n, n)
+        np.add.at(ref, gd, s[c] * d * (A @ (d * u[gd])))
+    scaled = np.zeros(o0.N)
+    scaled[:nf] = (Ka @ u - mm * (K0 @ u))[:nf]
+    direct = Kp @ x - K0 @ x
+    size = np.abs(ref).max()
+    assert np.abs(direct[nf:]).max() == 0.0  # divergence rows: theta-independent, bitwise equal
+    # measured: the scaled form within 6.5e-15 of ref relative to its size, the plain difference
+    # within 3.7e-9 (its rounding error is relative to K x, which is about 1e6 times larger)
+    assert np.abs(scaled - ref).max() <= 1e-13 * size
+    assert np.abs(direct - ref).max() <= 1e-13 * np.abs(K0 @ x).max()
