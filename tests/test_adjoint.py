@@ -6,6 +6,8 @@ Checks, with the tolerance of each written in the test:
   contraction lambda_E^T A_E u_E with the oracle's own dof map and signs): relative 1e-8;
 * against central finite differences (step 1e-6, 20 seeded unit directions) of J computed by the
   GPU solver at tolerance 1e-12: relative 1e-6 of the largest directional derivative;
+* against the same central differences with the numerator formed from the solution corrections
+  (no cancellation between two values of J): 1e-9 of the largest directional derivative;
 * against central finite differences (step 1e-6) of J computed by the oracle's direct solver (no
   Krylov error): 1e-6 of the gradient norm.
 """
@@ -107,6 +109,61 @@ def test_gradient_matches_central_differences(annulus2k):
             ad.append(float(g @ vt))
     ad, fd = np.array(ad), np.array(fd)
     assert np.abs(ad - fd).max() <= 1e-6 * np.abs(ad).max(), (ad, fd)
+    h.close()
+
+
+def test_gradient_matches_cancellation_free_differences(annulus2k):
+    """Central differences (step 1e-6) whose numerator J(+) - J(-) = sum_o (p+ - p-)(p+ + p- - 2 d_o)
+    is formed from the corrections e = x(theta +- step v) - x0, each solved for directly:
+    K(theta') e = (b - K(theta) x0) - (K(theta') - K(theta)) x0, the last term from the per-cell
+    scaling of the flux block (an apply of the flux part u0 at theta - log(s + m) less m times its
+    apply at theta, s = expm1(-+step v), m a power of two). Free of the rounding of two values of J,
+    so the bound is 1e-9 of the largest directional derivative (1e-6 for plain differences)."""
+    m, th, pts = annulus2k
+    h = vemgpu.DarcyGpu(m, k=0, geometry="arcs", problem="annulus", bc="pressure", theta=th)
+    obs = observe.PointObservation(h, m, pts, data=np.linspace(0.2, 0.8, len(pts)))
+    x0 = h.zeros()
+    try:
+        h.solve(x=x0, mode="fp64", tol=1e-13)
+    except vemgpu.VemGpuError:
+        pass  # the FP64 floor was reached first: x0 is the last iterate (checked below)
+    dJdx = torch.autograd.functional.vjp(obs, x0)[1]
+    g, _ = h.adjoint_grad(x0, dJdx, mode="fp64", tol=1e-12)
+    base = torch.tensor(th, dtype=torch.float64, device="cuda")
+    b0 = h.rhs()
+    r0 = b0 - h.apply(x0)
+    assert float(torch.linalg.norm(r0) / torch.linalg.norm(b0)) <= 1e-12
+    u0 = x0.clone()
+    u0[h.nf:] = 0
+    y0 = h.apply(u0)
+    res = obs.pressure(x0) - obs.data
+
+    def correction(v, sigma):
+        s = torch.expm1(-sigma * 1e-6 * v)
+        mm = 2.0 ** np.ceil(np.log2(2 * float(s.abs().max())))
+        h.set_log_permeability(base - torch.log(s + mm))
+        ya = h.apply(u0)
+        r = r0.clone()
+        r[:h.nf] -= ya[:h.nf] - mm * y0[:h.nf]
+        h.set_log_permeability(base + sigma * 1e-6 * v)
+        e = h.zeros()
+        try:
+            h.solve(b=r, x=e, mode="fp64", tol=1e-12)
+        except vemgpu.VemGpuError:
+            pass  # the FP64 floor was reached first: e is the last iterate
+        return obs.pressure(e)
+
+    rng = np.random.default_rng(35)
+    ad, fd = [], []
+    for _ in range(10):
+        v = torch.tensor(rng.standard_normal(len(th)), device="cuda")
+        v /= torch.linalg.norm(v)
+        dp, dm = correction(v, 1.0), correction(v, -1.0)
+        fd.append(float(((dp - dm) * (2 * res + dp + dm)).sum()) / 2e-6)
+        ad.append(float(g @ v))
+    h.set_log_permeability(base)
+    ad, fd = np.array(ad), np.array(fd)
+    assert np.abs(ad - fd).max() <= 1e-9 * np.abs(ad).max(), (ad, fd)
     h.close()
 
 
