@@ -1189,9 +1189,10 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
     else
         VG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
     double h_red[2] = {0, 0};
-    auto true_residual = [&]() {
+    // zero_x: x is the zero initial guess, K x = 0 and r = b without an apply
+    auto true_residual = [&](bool zero_x = false) {
         y.zero(s);
-        apply_int<double>(x, y.data(), cons, -1.0, s, nullptr);
+        if (!zero_x) apply_int<double>(x, y.data(), cons, -1.0, s, nullptr);
         residual64(bs.data(), y.data(), r.data(), N, d_red_.data(), d_partials_.data(), d_counter_.data(), s);
         n_launch += 1;
         VG_CUDA(cudaMemcpyAsync(h_red, d_red_.data(), sizeof(h_red), cudaMemcpyDeviceToHost, s));
@@ -1199,7 +1200,7 @@ void Solver::solve(const double* b, double* x, const vg_solve_opts& o, vg_solve_
         double nb = std::sqrt(h_red[1]);
         return std::sqrt(h_red[0]) / (nb > 0 ? nb : 1.0);
     };
-    double rel = true_residual();
+    double rel = true_residual(!o.nonzero_guess);
     int total = 0, outer = 0;
     const double nb = std::sqrt(h_red[1]) > 0 ? std::sqrt(h_red[1]) : 1.0;
     if (o.mode == VG_SOLVE_FP64) {
