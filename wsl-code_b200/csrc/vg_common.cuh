@@ -3,7 +3,11 @@
 //
 // Mathematics follows the reference GPU project (vem/CurvedVEM_Darcy_gpu/include/device.cuh:151-222,
 // include/problem_device.cuh:166-233) and its CPU modules (lib/polynomial_basis.cpp:95-293,
-// core/gauss_quadrature.cpp:74-305, examples/darcy_problem.h:70-121).
+// core/gauss_quadrature.cpp:74-305, examples/darcy_problem.h:70-121). The basis helpers below
+// (multi_index, mono, hdiv, binomial, edge_coeff, moment) are a deliberate restatement of the
+// reference's exponent / mono / basis / binom / edge_coeff / moment (device.cuh:159-222): they fix
+// the ordering and scaling of the monomial and H(div) degrees of freedom, which must be the same
+// for the discrete operator and the solution vectors to match the reference entry for entry.
 #pragma once
 #include <cuda_runtime.h>
 
