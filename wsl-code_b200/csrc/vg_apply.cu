@@ -13,8 +13,8 @@
 //   cells of one edge count, vg_common.cuh) is one contiguous record of the record stream
 //   (A_E, W_E, signed map and cell ids, lane-strided). Persistent CTAs own contiguous runs of
 //   records; one producer thread streams them with cp.async.bulk into a ring of shared-memory
-//   stages (mbarrier completion), consumer warps run the cell bodies out of shared memory and
-//   release each stage on an "empty" mbarrier. Bytes in flight are set by the ring, not by how
+//   stages (mbarrier completion), consumer warps (two groups, each owning alternate stages) run
+//   the cell bodies out of shared memory and release each stage on an "empty" mbarrier. Bytes in flight are set by the ring, not by how
 //   many warps fit on an SM, so the stream runs at HBM speed with few resident warps. Every
 //   wait is bounded (globaltimer); a wait that gives up sets an error word, drains the copies
 //   it issued and returns.
@@ -619,7 +619,8 @@ template <typename T>
 void launch_apply(ApplyArgs<T> a, cudaStream_t s) {
     if (a.rec && a.k <= 1) {
         if (a.ncta == 0) return;
-        if (a.stages < BULK_GROUPS || a.stages % BULK_GROUPS) throw Error(VG_EINVAL, "apply ring: stage count not a multiple of the consumer groups");
+        if (a.stages < BULK_GROUPS || a.stages % BULK_GROUPS)
+            throw Error(VG_EINVAL, "apply ring: stage count not a multiple of the consumer groups");
         const size_t smem = size_t(a.stages) * a.stage_bytes;
         if (a.k == 0)
             apply_bulk_kernel<T, 0><<<a.ncta, BULK_THREADS, smem, s>>>(a);
